@@ -1,0 +1,424 @@
+"""Benchmark of the B200 LBM engine's time step (MLUPS and HBM roofline).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload tortuous8|tortuous20|pipe] [--storage f32|f16|bf16|f64]
+
+Workload (default): the tortuous stenosed vessel in a 512 x 512 x 1024 box —
+sinusoidal centerline (amplitude 30 lu, wavelength 200 lu), Gaussian 50 %-area
+stenosis at mid-length, D3Q19, tau 0.52, plug inlet 0.05 lu — at the stated
+~8 % fluid fraction of the box (radius from fluid_fraction_radius). The
+vessel's own radius 20 lu gives ~0.6 % of the box; that variant is timed too
+and reported under "variants". Inputs are synthetic and seeded (none needed:
+the geometry is analytic and the initial state is f = w). The population
+state (>= 1.6 GB) is larger than L2 (126 MB), so no flush is needed between
+steps.
+
+A step is one time step over every fluid node: the boundary pre-pass (WSS of
+near-wall nodes, outlet sources) and the AA stream+collide kernel. `value`
+is fluid-node updates per second over all GPUs (MLUPS), timed with CUDA
+events on the engine's stream; `e2e` times the same through the C ABI from
+host buffers (state upload, steps, state and WSS download). With --gpus N
+(torchrun) every rank runs an independent replica: the path has no
+inter-GPU exchange on one domain ("replicas only").
+
+--impl reference times the reference solver's own step loop (built from its
+sources into oracle/_ref/refharness) on slabs of the same vessel, one process
+per host core, and prints the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "reza-seti_b200"))
+
+METRIC = "MLUPS"
+BYTES_PER_POP = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}
+TAU = 0.52
+INLET_VEL = 0.05
+BOX = (512, 512, 1024)
+
+
+def build_workload(name):
+    from lbm_b200 import geometry as G
+    if name == "tortuous8":
+        r = G.fluid_fraction_radius(0.08, BOX)
+        topo = G.tortuous_vessel(radius=r, box=BOX)
+        desc = "tortuous stenosed vessel, 512x512x1024 box, ~8% fluid (radius %.1f lu)" % r
+    elif name == "tortuous20":
+        r = 20.0
+        topo = G.tortuous_vessel(radius=r, box=BOX)
+        desc = "tortuous stenosed vessel, 512x512x1024 box, radius 20 lu"
+    elif name == "pipe":
+        r = 16.0
+        topo = G.straight_pipe(radius=r, length=136, box=(40, 40, 136))
+        desc = "straight pipe R=16 lu in a 40x40x136 box"
+    else:
+        raise SystemExit("unknown workload " + name)
+    return topo, desc, r
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic_per_node(storage):
+    """DRAM bytes per fluid node and launch of the step kernel, from the
+    committed ncu summary (profiles/step_kernel_d3q19.md), or None."""
+    path = os.path.join(ROOT, "profiles", "step_kernel_d3q19.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_node_%s:" % storage):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def time_engine(topo, storage, steps, warmup, device, torch):
+    from lbm_b200 import Engine
+    eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device)
+    eng.set_flow(False, INLET_VEL)
+    stream = torch.cuda.Stream(device=device)
+    eng.set_stream(stream.cuda_stream)
+    eng.step(warmup)
+    torch.cuda.synchronize(device)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    ms_step, ms_bnd = eng.step_timed(steps)
+    stop.record(stream)
+    stop.synchronize()
+    total_ms = start.elapsed_time(stop)
+    return eng, total_ms, ms_step, ms_bnd
+
+
+def run_gpu(args):
+    import torch
+    world, rank, local, dist = dist_setup(args.gpus)
+    device = local
+    torch.cuda.set_device(device)
+    topo, desc, radius = build_workload(args.workload)
+    n = len(topo["kind"])
+    storage = args.storage
+    S = BYTES_PER_POP[storage]
+    Q = 19
+
+    # headline: K steps on the engine stream, CUDA events, barrier + sync both sides
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clk:
+        eng, total_ms, ms_step, ms_bnd = time_engine(topo, storage, args.steps, args.warmup, device, torch)
+    torch.cuda.synchronize(device)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    clocks = clk.summary()
+    info = eng.info()
+    flags = eng.flags()
+    mlups = n * args.steps / (total_ms / 1e3) / 1e6 * world
+    ms_per_step = total_ms / args.steps
+
+    # roofline of the dominant kernel (stream+collide): algorithmic bytes 2 Q S per node
+    peak, peak_kind = measured_peaks()
+    alg_bytes = 2 * Q * S * n
+    step_avg_ms = ms_step / args.steps
+    achieved = alg_bytes / (step_avg_ms / 1e3) / 1e9
+    tpn = profile_traffic_per_node(storage)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": round(tpn * n) if tpn else None,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "step_kernel_ms": round(step_avg_ms, 5),
+                "boundary_kernel_ms": round(ms_bnd / args.steps, 5)}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        e2e = end_to_end(eng, n, Q, args.steps, torch)
+    eng.close()
+
+    variants = {}
+    if rank == 0 and not args.no_variants:
+        variants = run_variants(args, topo, n, torch, device)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference(args, sample_only=True)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f32": "f32 (storage f - w), f32 compute", "f16": "f16 storage, f32 compute",
+                      "bf16": "bf16 storage, f32 compute", "f64": "f64"}[storage],
+            "data": "synthetic (analytic vessel geometry, f = w initial state)",
+            "config": {"workload": desc, "lattice": "D3Q19", "fluid_nodes": n,
+                       "box_cells": BOX[0] * BOX[1] * BOX[2] if args.workload.startswith("tortuous") else None,
+                       "tau": TAU, "inlet_velocity": INLET_VEL, "storage": storage,
+                       "bc_mode": "reference", "segments": info["n_segments"],
+                       "near_wall_nodes": info["n_nearwall"],
+                       "l2": "state larger than L2 (no flush)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 2 * args.steps, "clocks": clocks, "device_flags": flags,
+            "variants": variants,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def end_to_end(eng, n, Q, steps, torch):
+    """State upload, `steps` steps and result download through the C ABI from
+    pinned host buffers, timed on the host clock around the synchronous calls."""
+    f = torch.empty((n, Q), dtype=torch.float64).pin_memory().numpy()
+    f[:] = eng.populations()
+    wss = torch.empty(eng.n_nearwall, dtype=torch.float64).pin_memory().numpy()
+    t0 = time.perf_counter()
+    eng.set_populations(f)
+    eng.step(steps)
+    eng.populations(out=f)
+    from lbm_b200 import capi
+    capi.check(capi.lib().lbm_get_wss(eng._h, wss.ctypes.data, None, None), eng._h)
+    dt = time.perf_counter() - t0
+    h2d = n * Q * 8
+    d2h = n * Q * 8 + eng.n_nearwall * 8
+    return {"value": round(n * steps / dt / 1e6, 1), "unit": "MLUPS",
+            "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
+            "seconds": round(dt, 4)}
+
+
+def run_variants(args, topo, n, torch, device):
+    out = {}
+    steps = max(10, args.steps // 2)
+    for storage in ("f16", "bf16", "f64"):
+        if storage == args.storage:
+            continue
+        eng, total_ms, ms_step, _ = time_engine(topo, storage, steps, args.warmup, device, torch)
+        S = BYTES_PER_POP[storage]
+        out[storage] = {"MLUPS": round(n * steps / (total_ms / 1e3) / 1e6, 1),
+                        "step_kernel_GBs": round(2 * 19 * S * n / (ms_step / steps / 1e3) / 1e9, 1)}
+        eng.close()
+    if args.workload == "tortuous8":
+        from lbm_b200 import geometry as G
+        t20 = G.tortuous_vessel(radius=20.0, box=BOX)
+        n20 = len(t20["kind"])
+        eng, total_ms, ms_step, _ = time_engine(t20, "f32", steps, args.warmup, device, torch)
+        out["radius20_f32"] = {"fluid_nodes": n20,
+                               "MLUPS": round(n20 * steps / (total_ms / 1e3) / 1e6, 1)}
+        eng.close()
+    return out
+
+
+# ------------------------------------------------------------ reference arm ---
+def write_nodemap(path, topo, zlo, zhi):
+    """Node-map file of the slab zlo <= z < zhi for the reference harness
+    (format documented in oracle/refharness/harness.cpp). The slab's last
+    layer becomes its outlet."""
+    c = topo["coords"]
+    sel = (c[:, 2] >= zlo) & (c[:, 2] < zhi)
+    cs = c[sel]
+    kind = topo["kind"][sel].astype(np.int64)
+    lo = cs.min(axis=0)
+    hi = cs.max(axis=0)
+    shape = hi - lo + 1
+    cls = np.zeros(tuple(shape), np.uint8)
+    code = np.array([1, 2, 4, 3])[kind]
+    top = cs[:, 2] == hi[2]
+    code[top & (kind != 1)] = 4
+    loc = cs - lo
+    cls[loc[:, 0], loc[:, 1], loc[:, 2]] = code
+    nw = topo["nearwall"]
+    nwc = c[nw]
+    msel = (nwc[:, 2] >= zlo) & (nwc[:, 2] < zhi)
+    with open(path, "wb") as fh:
+        fh.write(b"NMAP")
+        np.array([shape[0], shape[1], shape[2], 1], np.int32).tofile(fh)
+        np.array([1.0, 0, 0, 0, 0, 0, -1.0, 0, 0, 1.0], np.float64).tofile(fh)
+        cls.tofile(fh)
+        np.array([int(msel.sum())], np.int64).tofile(fh)
+        rec = np.zeros(int(msel.sum()), dtype=[("c", np.int32, 4), ("n", np.float64, 3)])
+        rec["c"][:, :3] = nwc[msel] - lo
+        rec["n"] = topo["nearwall_normal"][msel]
+        rec.tofile(fh)
+    return int(sel.sum())
+
+
+def cpu_reference(args, sample_only=False, steps=None, procs=None):
+    """Times the reference's own step loop on slabs of the workload, one
+    harness process per core; returns MLUPS over all processes."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "refharness")
+    if not os.path.exists(harness):
+        return {"value": None, "unit": "MLUPS", "unavailable": "oracle/_ref/refharness not built"}
+    topo, desc, _ = build_workload(args.workload)
+    ncores = os.cpu_count() or 1
+    procs = procs or (1 if sample_only else min(ncores, 32))
+    steps = steps or (8 if sample_only else max(3, args.steps // 10))
+    layers = 12
+    work = tempfile.mkdtemp()
+    cfg = os.path.join(work, "config.txt")
+    with open(cfg, "w") as fh:
+        fh.write("parameters:\n\n  FlowType: \"Constant\"\n  time_resolution: 1e-05\n"
+                 "  relaxation_factor: %r\n  grid_size: 0.5\n  CteVel: %r\n  MaxIter: %d\n"
+                 "  IterToWrite: 100000000\n\n" % (TAU, INLET_VEL, steps))
+    runs = []
+    nodes_total = 0
+    for p in range(procs):
+        zlo = p * layers
+        mp = os.path.join(work, "slab%d.bin" % p)
+        nodes_total += write_nodemap(mp, topo, zlo, zlo + layers)
+        runs.append(subprocess.Popen([harness, "nodemap", cfg, mp, str(steps), "-", "--time"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+    results = []
+    for r in runs:
+        out, _ = r.communicate()
+        for line in out.splitlines():
+            if line.startswith("{"):
+                results.append(json.loads(line))
+    if len(results) != procs:
+        return {"value": None, "unit": "MLUPS", "unavailable": "reference harness failed"}
+    # all processes run concurrently: aggregate = nodes / slowest wall time
+    slowest = max(r["seconds"] for r in results)
+    value = sum(r["nodes"] for r in results) * steps / slowest / 1e6
+    return {"value": round(value, 4), "unit": "MLUPS", "cores": procs, "kind": "reference",
+            "sample": "%d slab(s) of %d z-layers of the workload (%d nodes), %d steps each, "
+                      "reference Simulation step methods, serial MPI build"
+                      % (procs, layers, nodes_total, steps)}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    cpu = cpu_reference(args, sample_only=False)
+    if cpu.get("value") is None:
+        print(json.dumps({"impl": "reference", "unavailable": cpu.get("unavailable", "failed")}))
+        return
+    line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "MLUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (analytic vessel geometry, f = w initial state)",
+            "config": {"workload": build_workload(args.workload)[1], "lattice": "D3Q19",
+                       "tau": TAU, "inlet_velocity": INLET_VEL},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_seconds": round(time.perf_counter() - t0, 1)}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="engine")
+    ap.add_argument("--workload", default="tortuous8")
+    ap.add_argument("--storage", default="f32")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

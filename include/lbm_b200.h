@@ -1,0 +1,170 @@
+/*
+ * lbm_b200.h — C ABI of the B200 lattice-Boltzmann engine.
+ *
+ * The engine replaces the per-time-step loop of the reference solver
+ * (Simulation::Iterate, Simulation.cpp:538-618) on one GPU. A caller that
+ * holds the reference's SubDomain (its node list Involved_Lat_, the inlet /
+ * outlet / wall lists and the near-wall list with normals) flattens it once
+ * into an lbm_desc, creates an engine, and then drives time steps and reads
+ * results through these functions. Plain C types only; no exceptions cross
+ * the ABI; every function returns 0 on success or a negative lbm_status, and
+ * lbm_last_error() describes the last failure of a handle.
+ *
+ * Node order: every per-node array the caller passes or receives uses the
+ * caller's node order (for the reference, the order of Involved_Lat_,
+ * Subdomain.cpp:598-611); per-near-wall-node arrays use the order of the
+ * caller's near-wall list (SubDomain::nextToTheWall). Populations are in the
+ * reference's direction order (LatticeModel.cpp:92-192 for D3Q19), laid out
+ * [node][direction].
+ *
+ * Threading: one host thread per handle at a time. All device work of a
+ * handle runs on one CUDA stream (its own, or the one set with
+ * lbm_set_stream).
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lbm_engine lbm_engine;
+
+typedef enum {
+    LBM_OK = 0,
+    LBM_ERR_ARGUMENT = -1,    /* invalid argument or descriptor */
+    LBM_ERR_CUDA = -2,        /* a CUDA call failed */
+    LBM_ERR_NO_DEVICE = -3,   /* no CUDA device, or the kernels were not built for it */
+    LBM_ERR_STATE = -4,       /* call not valid in the engine's current state */
+    LBM_ERR_NUMERIC = -5      /* the device reported non-finite densities */
+} lbm_status;
+
+typedef enum { LBM_D3Q19 = 19, LBM_D3Q27 = 27 } lbm_lattice;
+
+/* Storage type of the populations. FP64 stores f and computes in FP64 with
+ * the reference's operand order; the others store f - w_q and compute in
+ * FP32. */
+typedef enum { LBM_STORE_F64 = 0, LBM_STORE_F32 = 1, LBM_STORE_F16 = 2, LBM_STORE_BF16 = 3 } lbm_storage;
+
+/* Boundary semantics.
+ * LBM_BC_REFERENCE: the reference's own rules — Zou-He plug inlet
+ *   (Boundary.cpp:111-289), zero-gradient outlet copy (Simulation.cpp:650-741),
+ *   wall-node fix-up (Simulation.cpp:746-763), wall nodes at rest in the
+ *   collision (Simulation.cpp:92-95). D3Q19 only.
+ * LBM_BC_PHYSICS: halfway bounce-back walls, velocity bounce-back inlet with a
+ *   per-node profile times a waveform factor, anti-bounce-back pressure outlet. */
+typedef enum { LBM_BC_REFERENCE = 0, LBM_BC_PHYSICS = 1 } lbm_bc_mode;
+
+/* Node kinds (Node::NodeType_ / Node::BoundaryType_, Struct.h:49-63). */
+typedef enum { LBM_NODE_FLUID = 0, LBM_NODE_INLET = 1, LBM_NODE_OUTLET = 2, LBM_NODE_WALL = 3 } lbm_node_kind;
+
+/* Flattened SubDomain. Replaces SubDomain's node graph (Subdomain.h:58-125):
+ * coordinates instead of neighbour pointers (the engine derives neighbours as
+ * SubDomain::Connectivity does, Subdomain.cpp:447-471), node kinds, and the
+ * boundary lists. Indices in the lists refer to the caller's node order. */
+typedef struct {
+    int32_t lattice;               /* lbm_lattice */
+    int32_t storage;               /* lbm_storage */
+    int32_t bc_mode;               /* lbm_bc_mode */
+    int32_t device;                /* CUDA device ordinal */
+    int64_t n_nodes;
+    const int32_t* coords;         /* [n_nodes][3] lattice coordinates (x_position...) */
+    const uint8_t* kind;           /* [n_nodes] lbm_node_kind */
+    int64_t n_inlet;
+    const int64_t* inlet;          /* InletBoundaryNode_.first */
+    double inlet_normal[3];        /* InletBoundaryNode_.second */
+    int32_t n_outlets;
+    const int64_t* outlet_offsets; /* [n_outlets + 1] into outlet_nodes */
+    const int64_t* outlet_nodes;   /* OutletBoundaryNodes_[k].first, concatenated */
+    const double* outlet_normals;  /* [n_outlets][3] OutletBoundaryNodes_[k].second */
+    int64_t n_wall;
+    const int64_t* wall;           /* WallBoundaryNode_ */
+    int64_t n_nearwall;
+    const int64_t* nearwall;       /* nextToTheWall */
+    const double* nearwall_normals;/* [n_nearwall][3] Node::normal */
+    double tau;                    /* relaxation time, Simulation::m_relaxation */
+    double dt;                     /* time step, Simulation::m_dt */
+    double spacing;                /* Geometry::spacing (mm), for the WSS scale */
+} lbm_desc;
+
+/* Flow types of Simulation::Iterate (Simulation.cpp:549-562). */
+typedef enum { LBM_FLOW_CONSTANT = 0, LBM_FLOW_PULSATILE = 1 } lbm_flow;
+
+/* Replaces Simulation(SubDomain&, SimulationParameters&) up to Iterate():
+ * flattens the node graph to device arrays and sets f = w (Node::Initialize,
+ * Node.cpp:71-78) and zero WSS accumulators (Simulation.cpp:66-71). */
+int lbm_create(const lbm_desc* desc, lbm_engine** out);
+int lbm_destroy(lbm_engine* e);
+
+/* Uses the given cudaStream_t (as void*) for all later device work. */
+int lbm_set_stream(lbm_engine* e, void* stream);
+
+/* Inlet velocity per step, as Iterate sets InletVelocity_ (Simulation.cpp:558-562):
+ * constant CteVel, or the pulsatile waveform of Simulation::getInletVelocity
+ * (:519-534) evaluated at the engine's flow clock, which starts at 0 and
+ * advances by dt per pulsatile step. */
+int lbm_set_flow(lbm_engine* e, int32_t flow, double cte_vel);
+
+/* Physics mode: inlet velocity per inlet node [n_inlet][3] (lattice units),
+ * multiplied each step by the waveform factor (1 for constant flow). */
+int lbm_set_inlet_profile(lbm_engine* e, const double* velocity);
+
+/* Physics mode: outlet density (default 1). */
+int lbm_set_outlet_density(lbm_engine* e, double rho);
+
+/* Runs n_steps time steps: for each, the work of Collision, Streaming,
+ * ApplyZouHeBc, ApplyOutletBc, ApplyWallBc, ComputeWallShearStress
+ * (Simulation.cpp:553-568). Asynchronous on the engine's stream; results
+ * below synchronise. */
+int lbm_step(lbm_engine* e, int64_t n_steps);
+
+/* Steps taken so far, and the flow clock (total_runtime). */
+int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime);
+
+/* Node::m_distributions after the last step (post-boundary populations),
+ * [n_nodes][q] in the caller's node order. */
+int lbm_get_populations(lbm_engine* e, double* f);
+
+/* Replaces the populations (the state after the current step); the next
+ * step collides them. */
+int lbm_set_populations(lbm_engine* e, const double* f);
+
+/* Node::density and Node::velocity after the last step: the moments the
+ * last step's collision used (Simulation.cpp:85-134). rho [n_nodes],
+ * u [n_nodes][3]; either may be NULL. */
+int lbm_get_macros(lbm_engine* e, double* rho, double* u);
+
+/* Near-wall outputs after the last step, in the caller's near-wall order:
+ * Node::wall_shear_stress, accumulated_shear_stress [3],
+ * accumulated_shear_stress_magnitude (Simulation.cpp:792-797). Any may be NULL. */
+int lbm_get_wss(lbm_engine* e, double* wss, double* acc, double* accmag);
+
+/* OSI and TAWSS from the accumulators (Simulation::ComputeOSIAndTAWSS,
+ * Simulation.cpp:804-826). Either may be NULL. */
+int lbm_get_osi_tawss(lbm_engine* e, double* osi, double* tawss);
+
+/* Device status bits since creation: 1 = a streamed population was exactly
+ * zero (the reference would not have streamed it), 2 = non-finite density. */
+int lbm_get_flags(lbm_engine* e, uint32_t* flags);
+
+/* Device time of the last n_steps steps run through lbm_step_timed, per kernel
+ * class: the stream+collide kernel and the boundary pre-pass (milliseconds,
+ * summed over the steps, CUDA events on the engine's stream). */
+int lbm_step_timed(lbm_engine* e, int64_t n_steps, double* step_kernel_ms, double* boundary_kernel_ms);
+
+/* Sizes: nodes, padded leading dimension, segments, near-wall nodes, outlet
+ * nodes, bytes of device memory held. Any may be NULL. */
+int lbm_get_info(lbm_engine* e, int64_t* n_nodes, int64_t* ld, int64_t* n_segments, int64_t* n_nearwall,
+                 int64_t* n_outlet_nodes, int64_t* device_bytes);
+
+/* Message of the last failed call on e (or of the last failed lbm_create when
+ * e is NULL). Never NULL. */
+const char* lbm_last_error(const lbm_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

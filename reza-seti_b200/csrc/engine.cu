@@ -1,0 +1,815 @@
+// Host side of the engine behind the C ABI (include/lbm_b200.h): flattens the
+// caller's node set into the device layout, owns the device buffers, and
+// sequences the kernels of each time step.
+//
+// Flattening (replaces the node graph SubDomain builds, Subdomain.cpp:364-611):
+//   * nodes are sorted x-major, z-fastest — the order of the reference's own
+//     Involved_Lat_ — so neighbours along z are adjacent and neighbours in
+//     other directions lie in neighbouring z-runs, which keeps every
+//     direction's accesses coalesced;
+//   * neighbours are found as SubDomain::Connectivity finds them (the node at
+//     x + c_q if it exists, Subdomain.cpp:447-471) through a column index of
+//     z-runs, and encoded as a per-node existence mask plus per-segment index
+//     offsets (lattice.cuh, Meta);
+//   * outlet copies are resolved to source nodes by replaying the reference's
+//     in-order sweep (Simulation.cpp:650-741): a node whose inward neighbour
+//     was already overwritten by the sweep reads that neighbour's source.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "lbm_b200.h"
+#include "launch.h"
+
+using namespace lbm;
+
+namespace {
+
+std::string g_create_error = "no error";
+
+struct Topo {
+    int n = 0;
+    long long ld = 0;
+    int nblocks = 0;
+    int nseg = 0;
+    std::vector<int> perm;   // internal -> caller
+    std::vector<int> iperm;  // caller -> internal
+    std::vector<uint64_t> meta;
+    std::vector<int> seg_base;
+    std::vector<int> seg_delta;
+    std::vector<int> aux;
+    std::vector<int> in_node;   // internal index per caller inlet entry
+    std::vector<int> out_node;  // internal index per outlet-table entry
+    std::vector<int> out_src;   // source node (internal) or -1
+    std::vector<float> out_nrm; // [n_out][3]
+    std::vector<int> nw_node;
+    std::vector<double> nw_normal;
+};
+
+struct ColumnIndex {
+    int x0 = 0, y0 = 0, nx = 0, ny = 0;
+    struct Run {
+        int z0, z1, start;
+    };
+    std::vector<int> col_first;
+    std::vector<Run> runs;
+    int lookup(int x, int y, int z) const {
+        if (x < x0 || y < y0 || x >= x0 + nx || y >= y0 + ny) return -1;
+        const long long c = (long long)(x - x0) * ny + (y - y0);
+        for (int r = col_first[c]; r < col_first[c + 1]; ++r)
+            if (z >= runs[r].z0 && z <= runs[r].z1) return runs[r].start + (z - runs[r].z0);
+        return -1;
+    }
+};
+
+template <int Q>
+std::string build_topology(const lbm_desc& d, Topo& t) {
+    using L = Lat<Q>;
+    using M = Meta<Q>;
+    if (d.n_nodes <= 0 || d.n_nodes > (long long)INT_MAX - BLOCK_NODES) return "n_nodes out of range";
+    if (!d.coords || !d.kind) return "coords and kind are required";
+    const int n = (int)d.n_nodes;
+    t.n = n;
+    t.nblocks = (n + BLOCK_NODES - 1) / BLOCK_NODES;
+    t.ld = (long long)t.nblocks * BLOCK_NODES;
+
+    // order: x-major, z-fastest
+    const int32_t* X = d.coords;
+    auto less = [X](int a, int b) {
+        if (X[3 * a] != X[3 * b]) return X[3 * a] < X[3 * b];
+        if (X[3 * a + 1] != X[3 * b + 1]) return X[3 * a + 1] < X[3 * b + 1];
+        return X[3 * a + 2] < X[3 * b + 2];
+    };
+    t.perm.resize(n);
+    std::iota(t.perm.begin(), t.perm.end(), 0);
+    if (!std::is_sorted(t.perm.begin(), t.perm.end(), less)) std::sort(t.perm.begin(), t.perm.end(), less);
+    t.iperm.assign(n, -1);
+    for (int i = 0; i < n; ++i) t.iperm[t.perm[i]] = i;
+    std::vector<int> cx(n), cy(n), cz(n), kind(n);
+    for (int i = 0; i < n; ++i) {
+        const int c = t.perm[i];
+        cx[i] = X[3 * c];
+        cy[i] = X[3 * c + 1];
+        cz[i] = X[3 * c + 2];
+        kind[i] = d.kind[c];
+        if (kind[i] > 3) return "node kind must be 0..3";
+        if (i && cx[i] == cx[i - 1] && cy[i] == cy[i - 1] && cz[i] == cz[i - 1]) return "duplicate node coordinates";
+    }
+
+    // column index of z-runs
+    ColumnIndex ci;
+    const int xmin = *std::min_element(cx.begin(), cx.end()), xmax = *std::max_element(cx.begin(), cx.end());
+    const int ymin = *std::min_element(cy.begin(), cy.end()), ymax = *std::max_element(cy.begin(), cy.end());
+    ci.x0 = xmin;
+    ci.y0 = ymin;
+    ci.nx = xmax - xmin + 1;
+    ci.ny = ymax - ymin + 1;
+    if ((long long)ci.nx * ci.ny > (1LL << 30)) return "node set spans too many (x, y) columns";
+    ci.col_first.assign((size_t)ci.nx * ci.ny + 1, 0);
+    std::vector<int> col_of_run;
+    for (int i = 0; i < n; ++i) {
+        const bool cont = i && cx[i] == cx[i - 1] && cy[i] == cy[i - 1] && cz[i] == cz[i - 1] + 1;
+        if (cont) {
+            ci.runs.back().z1 = cz[i];
+        } else {
+            ci.runs.push_back({cz[i], cz[i], i});
+            col_of_run.push_back((cx[i] - xmin) * ci.ny + (cy[i] - ymin));
+        }
+    }
+    for (int c : col_of_run) ci.col_first[c + 1]++;
+    for (size_t c = 0; c + 1 < ci.col_first.size(); ++c) ci.col_first[c + 1] += ci.col_first[c];
+
+    // metadata and segments
+    t.meta.assign(t.ld, 0);
+    t.seg_base.assign(t.nblocks + 1, 0);
+    t.seg_delta.clear();
+    t.aux.assign(t.ld, -1);
+    std::vector<char> defined(Q, 0);
+    int cur = -1;
+    int nb[Q];
+    for (int i = 0; i < n; ++i) {
+        uint64_t mask = 0;
+        for (int q = 0; q < Q; ++q) {
+            nb[q] = q == L::REST ? i : ci.lookup(cx[i] + L::cx(q), cy[i] + L::cy(q), cz[i] + L::cz(q));
+            if (nb[q] >= 0) mask |= 1ull << q;
+        }
+        bool fresh = cur < 0 || i % BLOCK_NODES == 0;
+        if (!fresh)
+            for (int q = 0; q < Q; ++q)
+                if (nb[q] >= 0 && defined[q] && t.seg_delta[(size_t)cur * Q + q] != nb[q] - i) {
+                    fresh = true;
+                    break;
+                }
+        if (fresh) {
+            cur = t.nseg++;
+            t.seg_delta.resize((size_t)t.nseg * Q, 0);
+            std::fill(defined.begin(), defined.end(), 0);
+            if (i % BLOCK_NODES == 0) t.seg_base[i / BLOCK_NODES] = cur;
+        }
+        for (int q = 0; q < Q; ++q)
+            if (nb[q] >= 0 && !defined[q]) {
+                t.seg_delta[(size_t)cur * Q + q] = nb[q] - i;
+                defined[q] = 1;
+            }
+        const uint64_t rel = (uint64_t)(cur - t.seg_base[i / BLOCK_NODES]);
+        if (rel >> M::SEG_BITS) return "segment index overflow";
+        t.meta[i] = mask | ((uint64_t)kind[i] << M::KIND_SHIFT) | (rel << M::SEG_SHIFT);
+    }
+    t.seg_base[t.nblocks] = t.nseg;
+
+    auto node_of = [&](int64_t caller, int want_kind, const char* what, std::string& err) -> int {
+        if (caller < 0 || caller >= n) {
+            err = std::string(what) + " index out of range";
+            return -1;
+        }
+        const int i = t.iperm[caller];
+        if (kind[i] != want_kind) {
+            err = std::string(what) + " list names a node of another kind";
+            return -1;
+        }
+        return i;
+    };
+    std::string err;
+
+    // inlet
+    if (d.n_inlet < 0 || (d.n_inlet > 0 && !d.inlet)) return "bad inlet list";
+    long long n_in_kind = 0, n_out_kind = 0;
+    for (int i = 0; i < n; ++i) {
+        n_in_kind += kind[i] == KIND_INLET;
+        n_out_kind += kind[i] == KIND_OUTLET;
+    }
+    if (d.n_inlet != n_in_kind) return "inlet list does not match the inlet node count";
+    for (int64_t k = 0; k < d.n_inlet; ++k) {
+        const int i = node_of(d.inlet[k], KIND_INLET, "inlet", err);
+        if (i < 0) return err;
+        if (t.aux[i] >= 0) return "node listed twice in the inlet list";
+        t.aux[i] = (int)k;
+        t.in_node.push_back(i);
+    }
+
+    // outlets, with the reference's in-order copy sweep resolved to sources
+    if (d.n_outlets < 0 || (d.n_outlets > 0 && (!d.outlet_offsets || !d.outlet_nodes || !d.outlet_normals)))
+        return "bad outlet description";
+    std::vector<int> src_of(n, -2);  // -2: not swept yet
+    for (int o = 0; o < d.n_outlets; ++o) {
+        const double* nr = d.outlet_normals + 3 * o;
+        int dd[3] = {0, 0, 0};
+        bool any = true;
+        if (nr[0] > 0) dd[0] = -1;
+        else if (nr[0] < 0) dd[0] = 1;
+        else if (nr[1] > 0) dd[1] = -1;
+        else if (nr[1] < 0) dd[1] = 1;
+        else if (nr[2] > 0) dd[2] = -1;
+        else if (nr[2] < 0) dd[2] = 1;
+        else any = false;
+        const int64_t b = d.outlet_offsets[o], e = d.outlet_offsets[o + 1];
+        if (b < 0 || e < b) return "bad outlet offsets";
+        for (int64_t k = b; k < e; ++k) {
+            const int i = node_of(d.outlet_nodes[k], KIND_OUTLET, "outlet", err);
+            if (i < 0) return err;
+            if (src_of[i] != -2) return "node listed twice in the outlet lists";
+            int src = -1;
+            if (any) {
+                const int m = ci.lookup(cx[i] + dd[0], cy[i] + dd[1], cz[i] + dd[2]);
+                if (m >= 0) src = (src_of[m] >= 0) ? src_of[m] : m;
+            }
+            src_of[i] = src;
+            t.aux[i] = (int)t.out_node.size();
+            t.out_node.push_back(i);
+            t.out_src.push_back(src);
+            for (int c = 0; c < 3; ++c) t.out_nrm.push_back((float)nr[c]);
+        }
+    }
+    if ((long long)t.out_node.size() != n_out_kind) return "outlet lists do not match the outlet node count";
+
+    // walls: only checked; the kernels use the node kind
+    if (d.n_wall < 0 || (d.n_wall > 0 && !d.wall)) return "bad wall list";
+    for (int64_t k = 0; k < d.n_wall; ++k)
+        if (node_of(d.wall[k], KIND_WALL, "wall", err) < 0) return err;
+
+    // near-wall nodes keep the caller's list order
+    if (d.n_nearwall < 0 || (d.n_nearwall > 0 && (!d.nearwall || !d.nearwall_normals))) return "bad near-wall list";
+    for (int64_t k = 0; k < d.n_nearwall; ++k) {
+        if (d.nearwall[k] < 0 || d.nearwall[k] >= n) return "near-wall index out of range";
+        t.nw_node.push_back(t.iperm[d.nearwall[k]]);
+        for (int c = 0; c < 3; ++c) t.nw_normal.push_back(d.nearwall_normals[3 * k + c]);
+    }
+    return "";
+}
+
+// Inlet waveform of the reference (Simulation::getInletVelocity,
+// Simulation.cpp:519-534, with the polynomial pieces of pulsatile.h:55-69),
+// evaluated on the host with the same expressions so the per-step velocity
+// equals the reference's.
+double waveform_piece(int piece, double x) {
+    if (piece == 1)
+        return (-8.579e+08 * std::pow(x, 8) + 4.059e+08 * std::pow(x, 7) - 7.817e+07 * std::pow(x, 6) +
+                7.994e+06 * std::pow(x, 5) - 4.835e+05 * std::pow(x, 4) + 1.782e+04 * std::pow(x, 3) -
+                321.6 * std::pow(x, 2) + 3.215 * x + 0.1423);
+    if (piece == 2)
+        return (-4.32e+06 * std::pow(x, 8) + 7.94e+06 * std::pow(x, 7) - 6.298e+06 * std::pow(x, 6) +
+                2.82e+06 * std::pow(x, 5) - 7.809e+05 * std::pow(x, 4) + 1.37e+05 * std::pow(x, 3) -
+                1.484e+04 * std::pow(x, 2) + 901.9 * x - 22.87);
+    return (-5.123 * std::pow(x, 4) + 14.15 * std::pow(x, 3) - 14.21 * std::pow(x, 2) + 5.865 * x - 0.5696);
+}
+
+double pulsatile_velocity(double t, double period) {
+    const double x = std::fmod(t, period);
+    if (x >= 0 && x < (0.1 * period)) return waveform_piece(1, x);
+    if (x >= (0.1 * period) && x < (0.3 * period)) return waveform_piece(2, x);
+    if (x >= (0.3 * period) && x < (0.9 * period)) return waveform_piece(3, x);
+    return 0.0;
+}
+
+template <class S, int Q>
+struct Tag {
+    using St = S;
+    static constexpr int q = Q;
+};
+
+}  // namespace
+
+struct lbm_engine {
+    std::string err = "no error";
+    int Q = 19, storage = 0, bc = 0, device = 0;
+    Topo t;
+    double tau = 1, omega = 1, dt = 0, spacing = 1, wss_c = 0;
+    double inlet_normal[3] = {0, 0, 0};
+    int flow = LBM_FLOW_CONSTANT;
+    double cte_vel = 0.0, out_rho = 1.0;
+    int64_t step = 0;
+    double runtime = 0.0;
+    int phase = 1;
+    int macro_buf = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+    // device buffers
+    void* pop = nullptr;
+    void* meta = nullptr;
+    int* seg_base = nullptr;
+    int* seg_delta = nullptr;
+    int* aux = nullptr;
+    int* out_src = nullptr;
+    void* out_buf = nullptr;
+    float* out_nrm = nullptr;
+    int* nw_node = nullptr;
+    double* nw_normal = nullptr;
+    double* nw_mom = nullptr;
+    double* wss = nullptr;
+    double* acc = nullptr;
+    double* accmag = nullptr;
+    double* obs_pop = nullptr;
+    double* obs_mom[2] = {nullptr, nullptr};
+    unsigned* flags = nullptr;
+    float* in_vel = nullptr;
+    int* perm = nullptr;
+    double* staging = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> evpool;
+
+    template <class T>
+    cudaError_t alloc(T** p, size_t count) {
+        const size_t b = std::max<size_t>(count, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc((void**)p, b);
+        if (e == cudaSuccess) {
+            allocs.push_back(*p);
+            bytes += b;
+        }
+        return e;
+    }
+    template <class T>
+    cudaError_t upload(T** p, const std::vector<T>& h) {
+        cudaError_t e = alloc(p, h.size());
+        if (e != cudaSuccess || h.empty()) return e;
+        return cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    }
+    int fail(int code, const std::string& msg) {
+        err = msg;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* where) {
+        err = std::string(where) + ": " + cudaGetErrorString(e);
+        return LBM_ERR_CUDA;
+    }
+    bool shifted() const { return storage != LBM_STORE_F64; }
+    int nw() const { return (int)t.nw_node.size(); }
+    int nout() const { return (int)t.out_node.size(); }
+    int nin() const { return (int)t.in_node.size(); }
+};
+
+namespace {
+
+template <class F>
+int dispatch(lbm_engine* e, F&& f) {
+    const bool q19 = e->Q == 19;
+    switch (e->storage) {
+        case LBM_STORE_F64: return q19 ? f(Tag<double, 19>{}) : f(Tag<double, 27>{});
+        case LBM_STORE_F32: return q19 ? f(Tag<float, 19>{}) : f(Tag<float, 27>{});
+        case LBM_STORE_F16: return q19 ? f(Tag<__half, 19>{}) : f(Tag<__half, 27>{});
+        default: return q19 ? f(Tag<__nv_bfloat16, 19>{}) : f(Tag<__nv_bfloat16, 27>{});
+    }
+}
+
+template <class S, int Q>
+StepArgs<S, Q> step_args(lbm_engine* e, double vel, float scale, double* mom) {
+    using C = typename Store<S>::C;
+    StepArgs<S, Q> a{};
+    a.pop = (S*)e->pop;
+    a.ld = e->t.ld;
+    a.n = e->t.n;
+    a.meta = (const typename Meta<Q>::T*)e->meta;
+    a.seg_base = e->seg_base;
+    a.seg_delta = e->seg_delta;
+    a.aux = e->aux;
+    a.omega = (C)e->omega;
+    for (int c = 0; c < 3; ++c) {
+        a.inlet_normal[c] = e->inlet_normal[c];
+        a.in_normal[c] = e->inlet_normal[c];
+    }
+    a.inlet_vel = vel;
+    a.out_src = e->out_src;
+    a.out_buf = (const C*)e->out_buf;
+    a.in_vel = e->in_vel;
+    a.in_scale = scale;
+    a.out_nrm = e->out_nrm;
+    a.out_rho = e->out_rho;
+    a.obs_pop = e->obs_pop;
+    a.obs_mom = mom;
+    a.flags = e->flags;
+    return a;
+}
+
+template <class S, int Q>
+BoundaryArgs<S, Q> boundary_args(lbm_engine* e, double vel) {
+    using C = typename Store<S>::C;
+    BoundaryArgs<S, Q> b{};
+    b.pop = (const S*)e->pop;
+    b.ld = e->t.ld;
+    b.meta = (const typename Meta<Q>::T*)e->meta;
+    b.seg_base = e->seg_base;
+    b.seg_delta = e->seg_delta;
+    b.n_nw = e->nw();
+    b.nw_node = e->nw_node;
+    b.nw_normal = e->nw_normal;
+    b.nw_mom = e->nw_mom;
+    b.wss = e->wss;
+    b.acc = e->acc;
+    b.accmag = e->accmag;
+    b.wss_c = e->wss_c;
+    b.n_out = e->bc == LBM_BC_REFERENCE ? e->nout() : 0;
+    b.out_src = e->out_src;
+    b.out_buf = (C*)e->out_buf;
+    for (int c = 0; c < 3; ++c) b.inlet_normal[c] = e->inlet_normal[c];
+    b.inlet_vel = vel;
+    return b;
+}
+
+// Collides the natural-layout state in obs_pop into the AA buffer and primes
+// the near-wall moments; the next step reads phase 1.
+int init_from_obs(lbm_engine* e) {
+    const int mb = (int)(e->step % 2);
+    int rc = dispatch(e, [&](auto tag) {
+        using S = typename decltype(tag)::St;
+        constexpr int Q = decltype(tag)::q;
+        auto a = step_args<S, Q>(e, 0.0, 0.f, e->obs_mom[mb]);
+        cudaError_t ce = launch_init<S, Q>(a, e->bc, e->stream);
+        return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "init kernel");
+    });
+    if (rc) return rc;
+    cudaError_t ce = launch_nearwall_moments(e->nw(), e->nw_node, e->obs_mom[mb], e->t.ld, e->shifted(),
+                                             e->nw_mom, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "near-wall moments");
+    e->phase = 1;
+    e->macro_buf = mb;
+    return 0;
+}
+
+int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
+    if (n_steps < 0) return e->fail(LBM_ERR_ARGUMENT, "negative step count");
+    if (n_steps == 0) return 0;
+    if (t_step) *t_step = 0;
+    if (t_bnd) *t_bnd = 0;
+    const bool timed = t_step || t_bnd;
+    // timed runs: events ev[2i] before the pre-pass of step i, ev[2i+1]
+    // before its stream+collide kernel, ev[2n] after the last step; read once
+    // at the end so timing adds no host round trip between steps
+    if (timed) {
+        if (n_steps > (1 << 20)) return e->fail(LBM_ERR_ARGUMENT, "too many timed steps in one call");
+        while ((int64_t)e->evpool.size() < 2 * n_steps + 1) {
+            cudaEvent_t ev;
+            cudaError_t ce = cudaEventCreate(&ev);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "event");
+            e->evpool.push_back(ev);
+        }
+    }
+    for (int64_t i = 0; i < n_steps; ++i) {
+        const int64_t t = e->step + 1;
+        const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
+        const double vel = pulsatile ? pulsatile_velocity(e->runtime, 0.9) : e->cte_vel;
+        const float scale = e->bc == LBM_BC_REFERENCE ? 0.f : (float)(pulsatile ? vel : 1.0);
+        int obs = 0;
+        if (i >= n_steps - 2) obs |= 2;
+        if (i == n_steps - 1) obs |= 1;
+        double* mom = e->obs_mom[t % 2];
+        const int phase = e->phase;
+        int rc = dispatch(e, [&](auto tag) {
+            using S = typename decltype(tag)::St;
+            constexpr int Q = decltype(tag)::q;
+            if (timed) cudaEventRecord(e->evpool[2 * i], e->stream);
+            cudaError_t ce = launch_boundary<S, Q>(boundary_args<S, Q>(e, vel), phase, e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "boundary kernel");
+            if (timed) cudaEventRecord(e->evpool[2 * i + 1], e->stream);
+            ce = launch_step<S, Q>(step_args<S, Q>(e, vel, scale, mom), phase, e->bc, obs, e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "step kernel");
+            return 0;
+        });
+        if (rc) return rc;
+        e->phase ^= 1;
+        e->step = t;
+        if (pulsatile) e->runtime += e->dt;
+    }
+    e->macro_buf = (int)((e->step - 1) % 2);
+    if (timed) {
+        cudaEventRecord(e->evpool[2 * n_steps], e->stream);
+        cudaError_t ce = cudaEventSynchronize(e->evpool[2 * n_steps]);
+        if (ce != cudaSuccess) return e->cuda_fail(ce, "timed steps");
+        double ms_step = 0, ms_bnd = 0;
+        for (int64_t i = 0; i < n_steps; ++i) {
+            float a = 0, b = 0;
+            cudaEventElapsedTime(&a, e->evpool[2 * i], e->evpool[2 * i + 1]);
+            cudaEventElapsedTime(&b, e->evpool[2 * i + 1], e->evpool[2 * i + 2]);
+            ms_bnd += a;
+            ms_step += b;
+        }
+        if (t_step) *t_step = ms_step;
+        if (t_bnd) *t_bnd = ms_bnd;
+    }
+    return 0;
+}
+
+int ensure_staging(lbm_engine* e) {
+    if (e->staging) return 0;
+    cudaError_t ce = e->alloc(&e->staging, (size_t)e->t.n * e->Q);
+    return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "staging buffer");
+}
+
+int sync(lbm_engine* e) {
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "stream synchronize");
+}
+
+int create(const lbm_desc* d, lbm_engine** out) {
+    if (!d || !out) {
+        g_create_error = "null descriptor or output pointer";
+        return LBM_ERR_ARGUMENT;
+    }
+    *out = nullptr;
+    if (d->lattice != 19 && d->lattice != 27) {
+        g_create_error = "lattice must be 19 or 27";
+        return LBM_ERR_ARGUMENT;
+    }
+    if (d->storage < 0 || d->storage > 3) {
+        g_create_error = "storage must be 0..3";
+        return LBM_ERR_ARGUMENT;
+    }
+    if (d->bc_mode != LBM_BC_REFERENCE && d->bc_mode != LBM_BC_PHYSICS) {
+        g_create_error = "bc_mode must be 0 or 1";
+        return LBM_ERR_ARGUMENT;
+    }
+    if (d->bc_mode == LBM_BC_REFERENCE && d->lattice != 19) {
+        g_create_error = "reference boundaries are defined for D3Q19 only (Boundary.cpp uses D3Q19 indices)";
+        return LBM_ERR_ARGUMENT;
+    }
+    if (!(d->tau > 0.5)) {
+        g_create_error = "tau must exceed 0.5";
+        return LBM_ERR_ARGUMENT;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_create_error = "no CUDA device";
+        return LBM_ERR_NO_DEVICE;
+    }
+    if (d->device < 0 || d->device >= ndev) {
+        g_create_error = "device ordinal out of range";
+        return LBM_ERR_ARGUMENT;
+    }
+    lbm_engine* e = new lbm_engine();
+    e->Q = d->lattice;
+    e->storage = d->storage;
+    e->bc = d->bc_mode;
+    e->device = d->device;
+    e->tau = d->tau;
+    e->omega = 1.0 / d->tau;
+    e->dt = d->dt;
+    e->spacing = d->spacing;
+    {
+        // Simulation::ComputeWallShearStress, Simulation.cpp:768-771
+        const double phys_den = 1060;
+        const double dtdt = d->dt * d->dt;
+        const double dxdx = d->spacing * d->spacing * 1e-6;
+        e->wss_c = phys_den * dtdt / dxdx;
+    }
+    for (int c = 0; c < 3; ++c) e->inlet_normal[c] = d->inlet_normal[c];
+    std::string msg = e->Q == 19 ? build_topology<19>(*d, e->t) : build_topology<27>(*d, e->t);
+    if (!msg.empty()) {
+        g_create_error = msg;
+        delete e;
+        return LBM_ERR_ARGUMENT;
+    }
+    auto bail = [&](cudaError_t ce, const char* where) {
+        g_create_error = std::string(where) + ": " + cudaGetErrorString(ce);
+        lbm_destroy(e);
+        return LBM_ERR_CUDA;
+    };
+    cudaError_t ce = cudaSetDevice(e->device);
+    if (ce != cudaSuccess) return bail(ce, "cudaSetDevice");
+    ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return bail(ce, "stream");
+    e->own_stream = true;
+    for (auto& ev : e->ev)
+        if ((ce = cudaEventCreate(&ev)) != cudaSuccess) return bail(ce, "event");
+
+    const Topo& t = e->t;
+    const size_t elem = e->storage == LBM_STORE_F64 ? 8 : (e->storage == LBM_STORE_F32 ? 4 : 2);
+    const size_t celem = e->storage == LBM_STORE_F64 ? 8 : 4;
+    char* p = nullptr;
+    if ((ce = e->alloc(&p, (size_t)e->Q * t.ld * elem)) != cudaSuccess) return bail(ce, "population buffer");
+    e->pop = p;
+    if (e->Q == 19) {
+        std::vector<uint32_t> m32(t.meta.begin(), t.meta.end());
+        uint32_t* mp = nullptr;
+        if ((ce = e->upload(&mp, m32)) != cudaSuccess) return bail(ce, "metadata");
+        e->meta = mp;
+    } else {
+        std::vector<unsigned long long> m64(t.meta.begin(), t.meta.end());
+        unsigned long long* mp = nullptr;
+        if ((ce = e->upload(&mp, m64)) != cudaSuccess) return bail(ce, "metadata");
+        e->meta = mp;
+    }
+    if ((ce = e->upload(&e->seg_base, t.seg_base)) != cudaSuccess) return bail(ce, "segments");
+    if ((ce = e->upload(&e->seg_delta, t.seg_delta)) != cudaSuccess) return bail(ce, "segments");
+    if ((ce = e->upload(&e->aux, t.aux)) != cudaSuccess) return bail(ce, "aux");
+    if ((ce = e->upload(&e->out_src, t.out_src)) != cudaSuccess) return bail(ce, "outlets");
+    if ((ce = e->upload(&e->out_nrm, t.out_nrm)) != cudaSuccess) return bail(ce, "outlets");
+    char* ob = nullptr;
+    if ((ce = e->alloc(&ob, (size_t)std::max(1, e->nout()) * e->Q * celem)) != cudaSuccess)
+        return bail(ce, "outlet buffer");
+    e->out_buf = ob;
+    if ((ce = e->upload(&e->nw_node, t.nw_node)) != cudaSuccess) return bail(ce, "near-wall");
+    if ((ce = e->upload(&e->nw_normal, t.nw_normal)) != cudaSuccess) return bail(ce, "near-wall");
+    if ((ce = e->alloc(&e->nw_mom, (size_t)4 * std::max(1, e->nw()))) != cudaSuccess) return bail(ce, "near-wall");
+    if ((ce = e->alloc(&e->wss, (size_t)e->nw())) != cudaSuccess) return bail(ce, "wss");
+    if ((ce = e->alloc(&e->acc, (size_t)3 * e->nw())) != cudaSuccess) return bail(ce, "wss");
+    if ((ce = e->alloc(&e->accmag, (size_t)e->nw())) != cudaSuccess) return bail(ce, "wss");
+    if ((ce = e->alloc(&e->obs_pop, (size_t)e->Q * t.ld)) != cudaSuccess) return bail(ce, "observation buffer");
+    for (auto& m : e->obs_mom)
+        if ((ce = e->alloc(&m, (size_t)4 * t.ld)) != cudaSuccess) return bail(ce, "observation buffer");
+    if ((ce = e->alloc(&e->flags, 1)) != cudaSuccess) return bail(ce, "flags");
+    std::vector<float> zero_in((size_t)3 * std::max(1, e->nin()), 0.f);
+    if ((ce = e->upload(&e->in_vel, zero_in)) != cudaSuccess) return bail(ce, "inlet profile");
+    if ((ce = e->upload(&e->perm, t.perm)) != cudaSuccess) return bail(ce, "permutation");
+
+    cudaMemsetAsync(e->wss, 0, sizeof(double) * std::max(1, e->nw()), e->stream);
+    cudaMemsetAsync(e->acc, 0, sizeof(double) * 3 * std::max(1, e->nw()), e->stream);
+    cudaMemsetAsync(e->accmag, 0, sizeof(double) * std::max(1, e->nw()), e->stream);
+    cudaMemsetAsync(e->flags, 0, sizeof(unsigned), e->stream);
+    // pad slots of the population buffer stay zero
+    cudaMemsetAsync(e->pop, 0, (size_t)e->Q * t.ld * elem, e->stream);
+    if ((ce = launch_fill_weights(e->obs_pop, t.ld, t.n, e->Q, e->stream)) != cudaSuccess)
+        return bail(ce, "initial state");
+    if (int rc = init_from_obs(e)) {
+        g_create_error = e->err;
+        lbm_destroy(e);
+        return rc;
+    }
+    if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) return bail(ce, "initialisation");
+    *out = e;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_create(const lbm_desc* desc, lbm_engine** out) {
+    try {
+        return create(desc, out);
+    } catch (const std::exception& ex) {
+        g_create_error = ex.what();
+        return LBM_ERR_ARGUMENT;
+    }
+}
+
+int lbm_destroy(lbm_engine* e) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (void* p : e->allocs) cudaFree(p);
+    for (auto& ev : e->ev)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ev : e->evpool) cudaEventDestroy(ev);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return 0;
+}
+
+int lbm_set_stream(lbm_engine* e, void* stream) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    e->own_stream = false;
+    e->stream = (cudaStream_t)stream;
+    return 0;
+}
+
+int lbm_set_flow(lbm_engine* e, int32_t flow, double cte_vel) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    if (flow != LBM_FLOW_CONSTANT && flow != LBM_FLOW_PULSATILE) return e->fail(LBM_ERR_ARGUMENT, "unknown flow type");
+    e->flow = flow;
+    e->cte_vel = cte_vel;
+    return 0;
+}
+
+int lbm_set_inlet_profile(lbm_engine* e, const double* velocity) {
+    if (!e || !velocity) return LBM_ERR_ARGUMENT;
+    std::vector<float> v((size_t)3 * e->nin());
+    for (size_t i = 0; i < v.size(); ++i) v[i] = (float)velocity[i];
+    if (v.empty()) return 0;
+    cudaSetDevice(e->device);
+    cudaError_t ce = cudaMemcpyAsync(e->in_vel, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "inlet profile");
+    return sync(e);
+}
+
+int lbm_set_outlet_density(lbm_engine* e, double rho) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    e->out_rho = rho;
+    return 0;
+}
+
+int lbm_step(lbm_engine* e, int64_t n_steps) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    return run_steps(e, n_steps, nullptr, nullptr);
+}
+
+int lbm_step_timed(lbm_engine* e, int64_t n_steps, double* step_kernel_ms, double* boundary_kernel_ms) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    double a = 0, b = 0;
+    int rc = run_steps(e, n_steps, &a, &b);
+    if (step_kernel_ms) *step_kernel_ms = a;
+    if (boundary_kernel_ms) *boundary_kernel_ms = b;
+    return rc;
+}
+
+int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    if (steps) *steps = e->step;
+    if (runtime) *runtime = e->runtime;
+    return 0;
+}
+
+int lbm_get_populations(lbm_engine* e, double* f) {
+    if (!e || !f) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    if (int rc = ensure_staging(e)) return rc;
+    cudaError_t ce = launch_pop_to_caller(e->obs_pop, e->perm, e->t.n, e->Q, e->t.ld, e->staging, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "reorder");
+    ce = cudaMemcpyAsync(f, e->staging, sizeof(double) * e->t.n * e->Q, cudaMemcpyDeviceToHost, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "download");
+    return sync(e);
+}
+
+int lbm_set_populations(lbm_engine* e, const double* f) {
+    if (!e || !f) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    if (int rc = ensure_staging(e)) return rc;
+    cudaError_t ce = cudaMemcpyAsync(e->staging, f, sizeof(double) * e->t.n * e->Q, cudaMemcpyHostToDevice, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "upload");
+    ce = launch_pop_from_caller(e->staging, e->perm, e->t.n, e->Q, e->t.ld, e->obs_pop, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "reorder");
+    if (int rc = init_from_obs(e)) return rc;
+    return sync(e);
+}
+
+int lbm_get_macros(lbm_engine* e, double* rho, double* u) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    if (int rc = ensure_staging(e)) return rc;
+    const int n = e->t.n;
+    double* r = e->staging;
+    double* uu = e->staging + n;
+    cudaError_t ce = launch_mom_to_caller(e->obs_mom[e->macro_buf], e->perm, n, e->t.ld, r, uu, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "reorder");
+    if (rho && (ce = cudaMemcpyAsync(rho, r, sizeof(double) * n, cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess)
+        return e->cuda_fail(ce, "download");
+    if (u && (ce = cudaMemcpyAsync(u, uu, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess)
+        return e->cuda_fail(ce, "download");
+    return sync(e);
+}
+
+int lbm_get_wss(lbm_engine* e, double* wss, double* acc, double* accmag) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    const size_t m = (size_t)e->nw();
+    cudaError_t ce = cudaSuccess;
+    if (wss && m) ce = cudaMemcpyAsync(wss, e->wss, sizeof(double) * m, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess && acc && m) ce = cudaMemcpyAsync(acc, e->acc, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess && accmag && m)
+        ce = cudaMemcpyAsync(accmag, e->accmag, sizeof(double) * m, cudaMemcpyDeviceToHost, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "download");
+    return sync(e);
+}
+
+int lbm_get_osi_tawss(lbm_engine* e, double* osi, double* tawss) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    const size_t m = (size_t)e->nw();
+    std::vector<double> acc(3 * m), accmag(m);
+    if (int rc = lbm_get_wss(e, nullptr, acc.data(), accmag.data())) return rc;
+    // Simulation::ComputeOSIAndTAWSS, Simulation.cpp:804-826 (period 0.9)
+    const double period = 0.9;
+    for (size_t k = 0; k < m; ++k) {
+        const double ta = accmag[k] / period;
+        const double norm = std::sqrt(std::pow(acc[3 * k], 2) + std::pow(acc[3 * k + 1], 2) + std::pow(acc[3 * k + 2], 2));
+        if (osi) osi[k] = 0.5 * (1.0 - (norm / accmag[k]));
+        if (tawss) tawss[k] = ta * e->dt;
+    }
+    return 0;
+}
+
+int lbm_get_flags(lbm_engine* e, uint32_t* flags) {
+    if (!e || !flags) return LBM_ERR_ARGUMENT;
+    cudaSetDevice(e->device);
+    unsigned v = 0;
+    cudaError_t ce = cudaMemcpyAsync(&v, e->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "download");
+    if (int rc = sync(e)) return rc;
+    *flags = v;
+    return 0;
+}
+
+int lbm_get_info(lbm_engine* e, int64_t* n_nodes, int64_t* ld, int64_t* n_segments, int64_t* n_nearwall,
+                 int64_t* n_outlet_nodes, int64_t* device_bytes) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    if (n_nodes) *n_nodes = e->t.n;
+    if (ld) *ld = e->t.ld;
+    if (n_segments) *n_segments = e->t.nseg;
+    if (n_nearwall) *n_nearwall = e->nw();
+    if (n_outlet_nodes) *n_outlet_nodes = e->nout();
+    if (device_bytes) *device_bytes = (int64_t)e->bytes;
+    return 0;
+}
+
+const char* lbm_last_error(const lbm_engine* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
+
+}  // extern "C"

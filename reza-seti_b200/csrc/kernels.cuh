@@ -1,0 +1,622 @@
+// Device code of the LBM engine: AA-pattern stream+collide kernels, the
+// boundary pre-pass (wall shear stress and outlet sources), initialisation and
+// reductions. Instantiated for each storage type in kernels_f64.cu (built
+// without FMA contraction, so FP64 results equal the reference's rounding)
+// and kernels_lowp.cu (FP32 / FP16 / BF16 storage, FP32 arithmetic).
+//
+// State layout in HBM: one population buffer pop[q * ld + n] (structure of
+// arrays, ld = node count padded to BLOCK_NODES), updated in place with the
+// AA access pattern. A kernel either reads the "natural" layout (phase 0:
+// slot (n, q) holds the population arriving at n in direction q) or the
+// "swapped" layout (phase 1: that population sits in slot (n - c_q, opp q)),
+// and leaves the other layout for the next step:
+//   phase 0: read slot (n, q);             write slot (n, opp q)
+//   phase 1: read slot (n - c_q, opp q);   write slot (n + c_q, q)
+// Every node reads and writes the same set of slots, so the in-place update
+// has no inter-thread hazard.
+//
+// Missing neighbours. In reference mode a population whose upstream node does
+// not exist keeps the value the node held before the step (the reference only
+// streams into existing neighbours, Simulation.cpp:247-251); the kernel keeps
+// that value in the slot the missing upstream would have written, which no
+// other thread touches. In physics mode the same slot receives the node's own
+// post-collision population in the opposite direction (halfway bounce-back),
+// with the velocity (inlet) or pressure (outlet) correction on open-boundary
+// links.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "lattice.cuh"
+
+namespace lbm {
+
+// ---------------------------------------------------------------- storage ---
+// Populations are stored as f (FP64) or as the deviation f - w_q from the
+// lattice weight (FP32 / FP16 / BF16), and computed in double or float.
+template <class S>
+struct Store;
+
+template <>
+struct Store<double> {
+    using C = double;
+    static constexpr bool SHIFTED = false;
+    __device__ static C get(const double* p) { return *p; }
+    __device__ static void put(double* p, C v) { *p = v; }
+};
+template <>
+struct Store<float> {
+    using C = float;
+    static constexpr bool SHIFTED = true;
+    __device__ static C get(const float* p) { return *p; }
+    __device__ static void put(float* p, C v) { *p = v; }
+};
+template <>
+struct Store<__half> {
+    using C = float;
+    static constexpr bool SHIFTED = true;
+    __device__ static C get(const __half* p) { return __half2float(*p); }
+    __device__ static void put(__half* p, C v) { *p = __float2half_rn(v); }
+};
+template <>
+struct Store<__nv_bfloat16> {
+    using C = float;
+    static constexpr bool SHIFTED = true;
+    __device__ static C get(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    __device__ static void put(__nv_bfloat16* p, C v) { *p = __float2bfloat16_rn(v); }
+};
+
+enum BcMode : int { BC_REFERENCE = 0, BC_PHYSICS = 1 };
+
+enum Flag : unsigned {
+    FLAG_ZERO_SKIP = 1u,  // a streamed population was exactly 0.0 (reference skips it)
+    FLAG_NONFINITE = 2u,  // a density became NaN or infinite
+};
+
+// ------------------------------------------------------------- arguments ---
+template <class S, int Q>
+struct StepArgs {
+    using C = typename Store<S>::C;
+    using MT = typename Meta<Q>::T;
+    S* pop;
+    long long ld;
+    int n;
+    const MT* meta;
+    const int* seg_base;   // [blocks] first segment of each block
+    const int* seg_delta;  // [segments][Q] neighbour index offsets
+    const int* aux;        // [n] index into the inlet / outlet tables (boundary kinds)
+    C omega;               // 1 / tau
+    // reference-mode inlet: one normal and one velocity for all inlet nodes
+    double inlet_normal[3];
+    double inlet_vel;
+    // reference-mode outlets: per outlet node, has-source flag and the
+    // populations copied from its source (written by the pre-pass)
+    const int* out_src;
+    const C* out_buf;
+    // physics-mode boundaries
+    const float* in_vel;   // [n_in][3] inlet velocity profile (lattice units)
+    float in_scale;        // waveform factor of this step
+    double in_normal[3];   // outward inlet normal
+    const float* out_nrm;  // [n_out][3] outward normal of each outlet node's outlet
+    double out_rho;        // outlet density
+    // observation (written only by observing launches)
+    double* obs_pop;       // [Q][ld] post-boundary populations f (natural layout)
+    double* obs_mom;       // [4][ld] rho, ux, uy, uz
+    unsigned* flags;
+};
+
+template <class S, int Q>
+struct BoundaryArgs {
+    using C = typename Store<S>::C;
+    using MT = typename Meta<Q>::T;
+    const S* pop;
+    long long ld;
+    const MT* meta;
+    const int* seg_base;
+    const int* seg_delta;
+    // near-wall nodes
+    int n_nw;
+    const int* nw_node;
+    const double* nw_normal;  // [n_nw][3]
+    double* nw_mom;           // [n_nw][4] moments of the previous step (rho or rho-1, u)
+    double* wss;              // [n_nw]
+    double* acc;              // [n_nw][3]
+    double* accmag;           // [n_nw]
+    double wss_c;             // 1060 dt^2 / (spacing^2 1e-6)
+    // outlet sources
+    int n_out;
+    const int* out_src;       // [n_out] source node or -1
+    C* out_buf;               // [n_out][Q]
+    double inlet_normal[3];
+    double inlet_vel;
+};
+
+// ------------------------------------------------------------ neighbours ---
+template <int Q>
+__device__ __forceinline__ const int* seg_row(const int* seg_base, const int* seg_delta, int n,
+                                              typename Meta<Q>::T m) {
+    const int s = __ldg(seg_base + n / BLOCK_NODES) + (int)(m >> Meta<Q>::SEG_SHIFT);
+    return seg_delta + (long long)s * Q;
+}
+
+// Populations arriving at node n (post-streaming values) in compute type.
+template <class S, int Q, int PHASE>
+__device__ __forceinline__ void gather(const S* __restrict__ pop, long long ld, int n,
+                                       typename Meta<Q>::T m, const int* sd,
+                                       typename Store<S>::C s[Q]) {
+    using L = Lat<Q>;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        long long idx;
+        if (PHASE == 0 || q == L::REST) {
+            idx = (long long)q * ld + n;
+        } else {
+            const int oq = L::opp(q);
+            idx = ((m >> oq) & 1) ? (long long)oq * ld + (n + __ldg(sd + oq)) : (long long)q * ld + n;
+        }
+        s[q] = Store<S>::get(pop + idx);
+    }
+}
+
+// --------------------------------------------------------------- moments ---
+// FP64, reference operand order (Simulation.cpp:85-139 for D3Q19).
+template <int Q>
+__device__ __forceinline__ void moments_ref(const double f[Q], bool wall, double& rho, double u[3]) {
+    using L = Lat<Q>;
+    rho = 0.0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) rho += f[q];
+    if (wall) {
+        u[0] = 0.0;
+        u[1] = 0.0;
+        u[2] = 0.0;
+        return;
+    }
+    if constexpr (Q == 19) {
+        u[0] = ((f[0] + f[6] + f[7] + f[8] + f[9]) - (f[1] + f[10] + f[11] + f[12] + f[13])) / rho;
+        u[1] = ((f[2] + f[6] + f[10] + f[14] + f[15]) - (f[3] + f[7] + f[11] + f[16] + f[17])) / rho;
+        u[2] = ((f[4] + f[8] + f[12] + f[14] + f[16]) - (f[5] + f[9] + f[13] + f[15] + f[17])) / rho;
+    } else {
+        double j[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (L::cx(q)) j[0] += L::cx(q) > 0 ? f[q] : -f[q];
+            if (L::cy(q)) j[1] += L::cy(q) > 0 ? f[q] : -f[q];
+            if (L::cz(q)) j[2] += L::cz(q) > 0 ? f[q] : -f[q];
+        }
+        u[0] = j[0] / rho;
+        u[1] = j[1] / rho;
+        u[2] = j[2] / rho;
+    }
+}
+
+// f_eq of direction q, reference operand order (Simulation.cpp:214-223).
+template <int Q>
+__device__ __forceinline__ double feq_ref(int q, double rho, const double u[3]) {
+    using L = Lat<Q>;
+    const double du = u[0] * (double)L::cx(q) + u[1] * (double)L::cy(q) + u[2] * (double)L::cz(q);
+    const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    return L::w(q) * rho * (1.0 + 3.0 * du + 4.5 * du * du - 1.5 * usq);
+}
+
+// FP32 arithmetic on deviations d_q = f_q - w_q: drho = rho - 1 = sum d,
+// momentum = sum c d (the weights carry no momentum).
+template <int Q>
+__device__ __forceinline__ void moments_shifted(const float d[Q], bool wall, float& drho, float u[3]) {
+    using L = Lat<Q>;
+    float a = 0.f, b = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) (q & 1 ? b : a) += d[q];
+    drho = a + b;
+    if (wall) {
+        u[0] = u[1] = u[2] = 0.f;
+        return;
+    }
+    float j[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (L::cx(q)) j[0] += L::cx(q) > 0 ? d[q] : -d[q];
+        if (L::cy(q)) j[1] += L::cy(q) > 0 ? d[q] : -d[q];
+        if (L::cz(q)) j[2] += L::cz(q) > 0 ? d[q] : -d[q];
+    }
+    const float inv = 1.f / (1.f + drho);
+    u[0] = j[0] * inv;
+    u[1] = j[1] * inv;
+    u[2] = j[2] * inv;
+}
+
+// deviation of f_eq from w_q
+template <int Q>
+__device__ __forceinline__ float deq_shifted(int q, float drho, const float u[3]) {
+    using L = Lat<Q>;
+    const float cu = u[0] * (float)L::cx(q) + u[1] * (float)L::cy(q) + u[2] * (float)L::cz(q);
+    const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    return (float)L::w(q) * (drho + (1.f + drho) * (3.f * cu + 4.5f * cu * cu - 1.5f * usq));
+}
+
+// BGK collision: c = s + omega (s_eq - s). Returns the moments it used:
+// m0 = rho (FP64) or rho - 1 (shifted), u.
+template <class C, int Q>
+__device__ __forceinline__ void collide(const C s[Q], bool wall, C omega, C c[Q], C& m0, C u[3]) {
+    if constexpr (sizeof(C) == 8) {
+        double rho;
+        moments_ref<Q>(s, wall, rho, u);
+        m0 = rho;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double fe = feq_ref<Q>(q, rho, u);
+            c[q] = s[q] + omega * (fe - s[q]);
+        }
+    } else {
+        float drho;
+        moments_shifted<Q>(s, wall, drho, u);
+        m0 = drho;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float de = deq_shifted<Q>(q, drho, u);
+            c[q] = s[q] + omega * (de - s[q]);
+        }
+    }
+}
+
+// ------------------------------------------------------------ Zou-He inlet ---
+// Velocity inlet of the reference, Boundary::ApplyBc (Boundary.cpp:111-289).
+// The six face branches are independent `if`s in the reference, applied in
+// this order. The rows keep its quirks: the y branches prescribe u_y = 1
+// (:178, :206) and the +z branch sums the -y population set (:239-241).
+struct ZouHeRow {
+    int comp, positive, vel_comp, unit_velocity;
+    int tang[9];
+    int out[5];
+    int denom_sign;
+    int nplus[2][3], nminus[2][3], nvcomp[2];
+    int dst[5], src[5], third[5], ca[5], sa[5], cb[5], sb[5], nidx[5], nsign[5];
+};
+
+__constant__ ZouHeRow kZouHe[6] = {
+    // +x (:115-140)
+    {0, 1, 0, 0, {2, 3, 4, 5, 14, 15, 16, 17, 18}, {0, 6, 7, 8, 9}, +1,
+     {{2, 14, 15}, {4, 16, 14}}, {{3, 16, 17}, {5, 15, 17}}, {1, 2},
+     {1, 10, 11, 13, 12}, {0, 7, 6, 8, 9}, {1, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
+     {-1, -1, -1, -1, -1}, {0, 1, 1, 2, 2}, {0, +1, -1, -1, +1}, {0, 0, 0, 1, 1},
+     {0, -1, +1, +1, -1}},
+    // -x (:143-168)
+    {0, 0, 0, 0, {2, 3, 4, 5, 14, 15, 16, 17, 18}, {1, 10, 11, 12, 13}, -1,
+     {{2, 14, 15}, {4, 16, 14}}, {{3, 16, 17}, {5, 15, 17}}, {1, 2},
+     {0, 7, 6, 8, 9}, {1, 10, 11, 13, 12}, {1, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
+     {+1, +1, +1, +1, +1}, {0, 1, 1, 2, 2}, {0, -1, +1, +1, -1}, {0, 0, 0, 1, 1},
+     {0, +1, -1, -1, +1}},
+    // +y (:171-195)
+    {1, 1, 1, 1, {0, 1, 4, 5, 8, 9, 12, 13, 18}, {2, 6, 10, 14, 15}, +1,
+     {{0, 8, 9}, {4, 8, 12}}, {{1, 12, 13}, {5, 9, 13}}, {0, 2},
+     {3, 11, 7, 17, 16}, {2, 6, 10, 14, 15}, {1, 0, 0, 0, 0}, {1, 0, 1, 1, 1},
+     {-1, -1, -1, -1, -1}, {0, 1, 0, 2, 2}, {0, -1, +1, -1, +1}, {0, 0, 0, 1, 1},
+     {0, +1, -1, +1, -1}},
+    // -y (:197-221)
+    {1, 0, 1, 1, {0, 1, 4, 5, 8, 9, 12, 13, 18}, {3, 7, 11, 16, 17}, -1,
+     {{0, 8, 9}, {4, 8, 12}}, {{1, 12, 13}, {5, 9, 13}}, {0, 2},
+     {2, 6, 10, 14, 15}, {3, 11, 7, 17, 16}, {1, 0, 0, 0, 0}, {1, 0, 1, 1, 1},
+     {+1, +1, +1, +1, +1}, {0, 1, 0, 2, 2}, {0, +1, -1, +1, -1}, {0, 0, 0, 1, 1},
+     {0, -1, +1, -1, +1}},
+    // +z (:225-249)
+    {2, 1, 2, 0, {0, 1, 4, 5, 8, 9, 12, 13, 18}, {3, 7, 11, 16, 17}, +1,
+     {{0, 6, 7}, {2, 6, 10}}, {{1, 10, 11}, {3, 7, 11}}, {0, 1},
+     {5, 9, 13, 15, 17}, {4, 12, 8, 16, 14}, {1, 0, 0, 0, 0}, {2, 0, 0, 1, 1},
+     {-1, +1, -1, +1, -1}, {0, 2, 2, 2, 2}, {0, -1, -1, -1, -1}, {0, 0, 0, 1, 1},
+     {0, -1, +1, -1, +1}},
+    // -z (:262-288)
+    {2, 0, 2, 0, {0, 1, 2, 3, 6, 7, 10, 11, 18}, {5, 9, 13, 15, 17}, -1,
+     {{0, 6, 7}, {2, 6, 10}}, {{1, 10, 11}, {3, 7, 11}}, {0, 1},
+     {4, 8, 12, 14, 16}, {5, 13, 9, 17, 15}, {1, 0, 0, 0, 0}, {2, 0, 0, 1, 1},
+     {+1, +1, -1, +1, -1}, {0, 2, 2, 2, 2}, {0, +1, +1, +1, +1}, {0, 0, 0, 1, 1},
+     {0, -1, +1, -1, +1}},
+};
+
+// Applies the reference Zou-He inlet to one node's D3Q19 populations s (f in
+// FP64, deviations f - w in the shifted types; the weights of every summed
+// set add up to 1 and cancel in every difference, so the same rows serve both).
+template <class C>
+__device__ __forceinline__ void zou_he(C s_in[19], const double normal[3], double vel) {
+    C f[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = s_in[q];
+    for (int b = 0; b < 6; ++b) {
+        const ZouHeRow& z = kZouHe[b];
+        const double nc = normal[z.comp];
+        if (!(z.positive ? nc > 0 : nc < 0)) continue;
+        C u[3] = {C(0), C(0), C(0)};
+        u[z.vel_comp] = z.unit_velocity ? C(1) : C(vel);
+        C tsum = f[z.tang[0]];
+        for (int k = 1; k < 9; ++k) tsum += f[z.tang[k]];
+        C osum = f[z.out[0]];
+        for (int k = 1; k < 5; ++k) osum += f[z.out[k]];
+        const C denom = z.denom_sign > 0 ? C(1) + u[z.vel_comp] : C(1) - u[z.vel_comp];
+        C rhoN;
+        if constexpr (sizeof(C) == 8) rhoN = (tsum + 2 * osum) / denom;
+        else rhoN = (C(1) + (tsum + 2 * osum)) / denom;
+        C N[2];
+        for (int c = 0; c < 2; ++c) {
+            const C d = f[z.nplus[c][0]] + f[z.nplus[c][1]] + f[z.nplus[c][2]] - f[z.nminus[c][0]] -
+                        f[z.nminus[c][1]] - f[z.nminus[c][2]];
+            N[c] = (C(1.0) / 2) * d - (C(1.0) / 3) * (rhoN * u[z.nvcomp[c]]);
+        }
+        for (int k = 0; k < 5; ++k) {
+            if (z.third[k]) {
+                const C t = (1 / C(3.0)) * rhoN * u[z.ca[k]];
+                f[z.dst[k]] = z.sa[k] > 0 ? f[z.src[k]] + t : f[z.src[k]] - t;
+            } else {
+                const C va = z.sa[k] > 0 ? u[z.ca[k]] : -u[z.ca[k]];
+                const C vb = z.sb[k] > 0 ? u[z.cb[k]] : -u[z.cb[k]];
+                const C t = f[z.src[k]] + (1 / C(6.0)) * rhoN * (va + vb);
+                f[z.dst[k]] = z.nsign[k] > 0 ? t + N[z.nidx[k]] : t - N[z.nidx[k]];
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) s_in[q] = f[q];
+}
+
+// Wall fix-up of the reference (Simulation.cpp:746-763): in direction order,
+// a missing neighbour in direction q copies the population of q into opp(q).
+template <class C, int Q>
+__device__ __forceinline__ void wall_fixup(C s[Q], typename Meta<Q>::T m) {
+    using L = Lat<Q>;
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        if (!((m >> q) & 1)) s[L::opp(q)] = s[q];
+}
+
+// ------------------------------------------------------ wall shear stress ---
+// Simulation::ComputeWallShearStress (Simulation.cpp:767-799), operand order
+// kept. fne[q] = f - f_eq of the near-wall node.
+template <class C, int Q>
+__device__ __forceinline__ void shear_traction(const C fne[Q], const double nrm_d[3], double wss_c,
+                                               double tau[3]) {
+    using L = Lat<Q>;
+    const C nrm[3] = {C(nrm_d[0]), C(nrm_d[1]), C(nrm_d[2])};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        C sum_alpha = C(0);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const C c[3] = {C(L::cx(q)), C(L::cy(q)), C(L::cz(q))};
+            C sum_k = C(0);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) sum_k += c[b] * nrm[b] * nrm[a];
+            C sum_j = C(0);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) sum_j += c[b] * nrm[b] * (c[a] - sum_k);
+            sum_alpha += fne[q] * sum_j;
+        }
+        tau[a] = wss_c * (double)sum_alpha;
+    }
+}
+
+// ---------------------------------------------------------------- kernels ---
+// One AA step over all nodes. BC selects reference or physics boundaries;
+// OBS writes the post-boundary populations and/or moments for the host.
+template <class S, int Q, int PHASE, int BC, int OBS>
+__global__ void __launch_bounds__(BLOCK_NODES) step_kernel(StepArgs<S, Q> a) {
+    using L = Lat<Q>;
+    using C = typename Store<S>::C;
+    using MT = typename Meta<Q>::T;
+    const int n = blockIdx.x * BLOCK_NODES + threadIdx.x;
+    if (n >= a.n) return;
+    const MT m = a.meta[n];
+    const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    const int* sd = nullptr;
+    if (PHASE == 1) sd = seg_row<Q>(a.seg_base, a.seg_delta, n, m);
+
+    C s[Q];
+    gather<S, Q, PHASE>(a.pop, a.ld, n, m, sd, s);
+
+    if constexpr (BC == BC_REFERENCE) {
+        if constexpr (!Store<S>::SHIFTED) {
+            // the reference does not stream a population that is exactly 0.0
+            // (Simulation.cpp:249); flag it, the AA layout cannot keep both values
+            bool zero = false;
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                if (q == L::REST || ((m >> L::opp(q)) & 1)) zero |= (s[q] == 0.0);
+            if (zero) atomicOr(a.flags, FLAG_ZERO_SKIP);
+        }
+        if (kind == KIND_INLET) {
+            if constexpr (Q == 19) zou_he<C>(s, a.inlet_normal, a.inlet_vel);
+        } else if (kind == KIND_OUTLET) {
+            const int k = a.aux[n];
+            if (a.out_src[k] >= 0) {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) s[q] = a.out_buf[(long long)k * Q + q];
+            }
+        } else if (kind == KIND_WALL) {
+            wall_fixup<C, Q>(s, m);
+        }
+    }
+
+    if (OBS & 1) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            a.obs_pop[(long long)q * a.ld + n] = Store<S>::SHIFTED ? (double)s[q] + L::w(q) : (double)s[q];
+    }
+
+    C c[Q], m0, u[3];
+    collide<C, Q>(s, BC == BC_REFERENCE && kind == KIND_WALL, a.omega, c, m0, u);
+    if (!isfinite((double)m0)) atomicOr(a.flags, FLAG_NONFINITE);
+
+    if (OBS & 2) {
+        a.obs_mom[n] = Store<S>::SHIFTED ? 1.0 + (double)m0 : (double)m0;
+        a.obs_mom[a.ld + n] = (double)u[0];
+        a.obs_mom[2 * a.ld + n] = (double)u[1];
+        a.obs_mom[3 * a.ld + n] = (double)u[2];
+    }
+
+    // Values for links whose far end is missing: reference mode keeps the
+    // node's own pre-collision value of the opposite direction; physics mode
+    // bounces the post-collision population back, corrected on inlet and
+    // outlet links.
+    C back[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if constexpr (BC == BC_REFERENCE) {
+            back[q] = s[L::opp(q)];
+        } else {
+            C v = c[q];
+            if (kind == KIND_INLET || kind == KIND_OUTLET) {
+                double nrm[3];
+                if (kind == KIND_INLET) {
+                    nrm[0] = a.in_normal[0], nrm[1] = a.in_normal[1], nrm[2] = a.in_normal[2];
+                } else {
+                    const float* o = a.out_nrm + 3 * (long long)a.aux[n];
+                    nrm[0] = o[0], nrm[1] = o[1], nrm[2] = o[2];
+                }
+                const double cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
+                if (cn > 0.0) {
+                    if (kind == KIND_INLET) {
+                        const int k = a.aux[n];
+                        const C uw[3] = {C(a.in_vel[3 * k] * a.in_scale), C(a.in_vel[3 * k + 1] * a.in_scale),
+                                         C(a.in_vel[3 * k + 2] * a.in_scale)};
+                        const C cu = L::cx(q) * uw[0] + L::cy(q) * uw[1] + L::cz(q) * uw[2];
+                        v = c[q] - C(6.0 * L::w(q)) * cu;
+                    } else {
+                        const C cu = L::cx(q) * u[0] + L::cy(q) * u[1] + L::cz(q) * u[2];
+                        const C usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+                        const C eq = C(1) + C(4.5) * cu * cu - C(1.5) * usq;
+                        if constexpr (Store<S>::SHIFTED)
+                            v = -c[q] + C(2.0 * L::w(q)) * (C(a.out_rho) * eq - C(1));
+                        else
+                            v = -c[q] + C(2.0 * L::w(q) * a.out_rho) * eq;
+                    }
+                }
+            }
+            back[q] = v;
+        }
+    }
+
+    if (PHASE == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int oq = L::opp(q);
+            const C v = (q == L::REST || ((m >> q) & 1)) ? c[q] : back[q];
+            Store<S>::put(a.pop + (long long)oq * a.ld + n, v);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (q == L::REST) {
+                Store<S>::put(a.pop + (long long)q * a.ld + n, c[q]);
+            } else {
+                if ((m >> q) & 1) Store<S>::put(a.pop + (long long)q * a.ld + (n + __ldg(sd + q)), c[q]);
+                const int oq = L::opp(q);
+                // slot (n, oq) is free when the node n - c_oq = n + c_q is missing
+                if (!((m >> q) & 1)) Store<S>::put(a.pop + (long long)oq * a.ld + n, back[q]);
+            }
+        }
+    }
+}
+
+// Initialisation from natural-layout populations f (double) in obs_pop: one
+// collision and a phase-0 store, so the next step reads phase 1. Writes the
+// moments of the given state to obs_mom.
+template <class S, int Q, int BC>
+__global__ void __launch_bounds__(BLOCK_NODES) init_kernel(StepArgs<S, Q> a) {
+    using L = Lat<Q>;
+    using C = typename Store<S>::C;
+    using MT = typename Meta<Q>::T;
+    const int n = blockIdx.x * BLOCK_NODES + threadIdx.x;
+    if (n >= a.n) return;
+    const MT m = a.meta[n];
+    const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    C s[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double f = a.obs_pop[(long long)q * a.ld + n];
+        s[q] = Store<S>::SHIFTED ? (C)(f - L::w(q)) : (C)f;
+        // round through the storage type so every later step sees stored values
+        S tmp;
+        Store<S>::put(&tmp, s[q]);
+        s[q] = Store<S>::get(&tmp);
+    }
+    C c[Q], m0, u[3];
+    collide<C, Q>(s, BC == BC_REFERENCE && kind == KIND_WALL, a.omega, c, m0, u);
+    a.obs_mom[n] = Store<S>::SHIFTED ? 1.0 + (double)m0 : (double)m0;
+    a.obs_mom[a.ld + n] = (double)u[0];
+    a.obs_mom[2 * a.ld + n] = (double)u[1];
+    a.obs_mom[3 * a.ld + n] = (double)u[2];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int oq = L::opp(q);
+        C v = c[q];
+        if (q != L::REST && !((m >> q) & 1)) v = BC == BC_REFERENCE ? s[oq] : c[q];
+        Store<S>::put(a.pop + (long long)oq * a.ld + n, v);
+    }
+}
+
+// Boundary pre-pass of one reference-mode step, before the step kernel of the
+// same phase: wall shear stress of near-wall nodes from the arriving
+// populations and the previous step's moments, and the source populations of
+// every outlet node (post-streaming, post-inlet values of the node the
+// reference's in-order copy sweep ends up reading).
+template <class S, int Q, int PHASE>
+__global__ void boundary_kernel(BoundaryArgs<S, Q> a) {
+    using C = typename Store<S>::C;
+    using MT = typename Meta<Q>::T;
+    using L = Lat<Q>;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.n_nw) {
+        const int n = a.nw_node[i];
+        const MT m = a.meta[n];
+        const int* sd = PHASE == 1 ? seg_row<Q>(a.seg_base, a.seg_delta, n, m) : nullptr;
+        C s[Q];
+        gather<S, Q, PHASE>(a.pop, a.ld, n, m, sd, s);
+        const double* mom = a.nw_mom + 4 * (long long)i;
+        C fne[Q];
+        if constexpr (sizeof(C) == 8) {
+            const double u[3] = {mom[1], mom[2], mom[3]};
+#pragma unroll
+            for (int q = 0; q < Q; ++q) fne[q] = s[q] - feq_ref<Q>(q, mom[0], u);
+        } else {
+            const float u[3] = {(float)mom[1], (float)mom[2], (float)mom[3]};
+#pragma unroll
+            for (int q = 0; q < Q; ++q) fne[q] = s[q] - deq_shifted<Q>(q, (float)mom[0], u);
+        }
+        double tau[3];
+        shear_traction<C, Q>(fne, a.nw_normal + 3 * (long long)i, a.wss_c, tau);
+        const double w = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
+        a.wss[i] = w;
+        a.acc[3 * (long long)i] += tau[0];
+        a.acc[3 * (long long)i + 1] += tau[1];
+        a.acc[3 * (long long)i + 2] += tau[2];
+        a.accmag[i] += w;
+        // moments of this step's collision input, for the next step's f_eq
+        C m0, u[3];
+        if constexpr (sizeof(C) == 8) {
+            double rho;
+            moments_ref<Q>(s, false, rho, u);
+            m0 = rho;
+        } else {
+            moments_shifted<Q>(s, false, m0, u);
+        }
+        double* mo = a.nw_mom + 4 * (long long)i;
+        mo[0] = (double)m0;
+        mo[1] = (double)u[0];
+        mo[2] = (double)u[1];
+        mo[3] = (double)u[2];
+    } else if (i < a.n_nw + a.n_out) {
+        const int k = i - a.n_nw;
+        const int n = a.out_src[k];
+        if (n < 0) return;
+        const MT m = a.meta[n];
+        const int* sd = PHASE == 1 ? seg_row<Q>(a.seg_base, a.seg_delta, n, m) : nullptr;
+        C s[Q];
+        gather<S, Q, PHASE>(a.pop, a.ld, n, m, sd, s);
+        if constexpr (Q == 19) {
+            if ((int)((m >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET) zou_he<C>(s, a.inlet_normal, a.inlet_vel);
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) a.out_buf[(long long)k * Q + q] = s[q];
+    }
+}
+
+}  // namespace lbm

@@ -1,0 +1,96 @@
+"""ctypes binding of the engine's C ABI (include/lbm_b200.h).
+
+Loads the in-tree liblbm_b200.so built by ``make -C reza-seti_b200``. There is
+no fallback: if the library is missing or cannot load, import fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "liblbm_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(PKG_DIR), "include", "lbm_b200.h")
+
+LBM_OK = 0
+LBM_ERR_ARGUMENT = -1
+LBM_ERR_CUDA = -2
+LBM_ERR_NO_DEVICE = -3
+LBM_ERR_STATE = -4
+LBM_ERR_NUMERIC = -5
+
+STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
+BC_REFERENCE, BC_PHYSICS = 0, 1
+FLOW_CONSTANT, FLOW_PULSATILE = 0, 1
+FLAG_ZERO_SKIP, FLAG_NONFINITE = 1, 2
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class LbmDesc(ctypes.Structure):
+    _fields_ = [
+        ("lattice", ctypes.c_int32), ("storage", ctypes.c_int32), ("bc_mode", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("n_nodes", ctypes.c_int64), ("coords", _i32p),
+        ("kind", _u8p), ("n_inlet", ctypes.c_int64), ("inlet", _i64p),
+        ("inlet_normal", ctypes.c_double * 3), ("n_outlets", ctypes.c_int32),
+        ("outlet_offsets", _i64p), ("outlet_nodes", _i64p), ("outlet_normals", _f64p),
+        ("n_wall", ctypes.c_int64), ("wall", _i64p), ("n_nearwall", ctypes.c_int64),
+        ("nearwall", _i64p), ("nearwall_normals", _f64p), ("tau", ctypes.c_double),
+        ("dt", ctypes.c_double), ("spacing", ctypes.c_double),
+    ]
+
+
+class LbmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("lbm error %d: %s" % (code, msg))
+        self.code = code
+
+
+_lib = None
+
+# name -> (restype, argtypes); mirrors include/lbm_b200.h
+_E = ctypes.c_void_p
+SIGNATURES = {
+    "lbm_create": (ctypes.c_int, [ctypes.POINTER(LbmDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "lbm_destroy": (ctypes.c_int, [_E]),
+    "lbm_set_stream": (ctypes.c_int, [_E, ctypes.c_void_p]),
+    "lbm_set_flow": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_double]),
+    "lbm_set_inlet_profile": (ctypes.c_int, [_E, _f64p]),
+    "lbm_set_outlet_density": (ctypes.c_int, [_E, ctypes.c_double]),
+    "lbm_step": (ctypes.c_int, [_E, ctypes.c_int64]),
+    "lbm_get_time": (ctypes.c_int, [_E, _i64p, _f64p]),
+    "lbm_get_populations": (ctypes.c_int, [_E, ctypes.c_void_p]),
+    "lbm_set_populations": (ctypes.c_int, [_E, ctypes.c_void_p]),
+    "lbm_get_macros": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),
+    "lbm_get_wss": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "lbm_get_osi_tawss": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),
+    "lbm_get_flags": (ctypes.c_int, [_E, ctypes.POINTER(ctypes.c_uint32)]),
+    "lbm_step_timed": (ctypes.c_int, [_E, ctypes.c_int64, _f64p, _f64p]),
+    "lbm_get_info": (ctypes.c_int, [_E, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),
+    "lbm_last_error": (ctypes.c_char_p, [_E]),
+}
+
+
+def lib():
+    """The loaded engine library (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("liblbm_b200.so is not built: run `make -C reza-seti_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code, handle=None):
+    if code != LBM_OK:
+        msg = lib().lbm_last_error(handle)
+        raise LbmError(code, msg.decode() if msg else "")
+    return code

@@ -1,0 +1,216 @@
+"""Python host mirror of the reference's time-step interface over the C ABI.
+
+``Engine`` wraps one lbm_engine handle. ``Simulation`` mirrors the reference's
+Simulation class (Simulation.h:54-90): it is built from a flattened SubDomain
+and a parameter set, and ``Iterate()`` runs the reference's loop with its stop
+rules (Simulation.cpp:549-550): MaxIter steps for constant flow, or while the
+flow clock is <= 2.7 for pulsatile flow.
+
+A topology is a dict of numpy arrays in the caller's node order, with the keys
+    coords [N,3], kind [N] (0 fluid, 1 inlet, 2 outlet, 3 wall),
+    inlet, inlet_normal [3], outlet_<k>, outlet_normal_<k> [3], wall,
+    nearwall, nearwall_normal [n,3]
+— the same keys the reference harness dumps.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import capi
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def outlets_of(topo):
+    outs, normals = [], []
+    k = 0
+    while "outlet_%d" % k in topo:
+        outs.append(np.asarray(topo["outlet_%d" % k], dtype=np.int64))
+        normals.append(np.asarray(topo["outlet_normal_%d" % k], dtype=np.float64).reshape(3))
+        k += 1
+    return outs, normals
+
+
+class Engine:
+    """One engine on one GPU."""
+
+    def __init__(self, topo, *, tau, dt=1e-5, spacing=1.0, lattice=19, storage="f64",
+                 bc="reference", device=0):
+        L = capi.lib()
+        self.q = lattice
+        keep = {}
+        keep["coords"] = np.ascontiguousarray(topo["coords"], dtype=np.int32).reshape(-1, 3)
+        keep["kind"] = np.ascontiguousarray(topo["kind"], dtype=np.uint8)
+        keep["inlet"] = np.ascontiguousarray(topo["inlet"], dtype=np.int64)
+        outs, normals = outlets_of(topo)
+        keep["outlet_offsets"] = np.concatenate([[0], np.cumsum([len(o) for o in outs])]).astype(np.int64)
+        keep["outlet_nodes"] = np.ascontiguousarray(
+            np.concatenate(outs) if outs else np.zeros(0), dtype=np.int64)
+        keep["outlet_normals"] = np.ascontiguousarray(np.array(normals, dtype=np.float64).reshape(-1))
+        keep["wall"] = np.ascontiguousarray(topo.get("wall", np.zeros(0)), dtype=np.int64)
+        keep["nearwall"] = np.ascontiguousarray(topo.get("nearwall", np.zeros(0)), dtype=np.int64)
+        keep["nearwall_normal"] = np.ascontiguousarray(
+            np.asarray(topo.get("nearwall_normal", np.zeros((0, 3))), dtype=np.float64).reshape(-1))
+        self.n = len(keep["kind"])
+        self.n_nearwall = len(keep["nearwall"])
+        self.n_inlet = len(keep["inlet"])
+        d = capi.LbmDesc()
+        d.lattice = lattice
+        d.storage = capi.STORAGE[storage]
+        d.bc_mode = capi.BC_REFERENCE if bc == "reference" else capi.BC_PHYSICS
+        d.device = device
+        d.n_nodes = self.n
+        d.coords = _p(keep["coords"], capi._i32p)
+        d.kind = _p(keep["kind"], capi._u8p)
+        d.n_inlet = self.n_inlet
+        d.inlet = _p(keep["inlet"], capi._i64p)
+        inl = np.asarray(topo.get("inlet_normal", np.zeros(3)), dtype=np.float64).reshape(-1)
+        for i in range(3):
+            d.inlet_normal[i] = float(inl[i]) if len(inl) == 3 else 0.0
+        d.n_outlets = len(outs)
+        d.outlet_offsets = _p(keep["outlet_offsets"], capi._i64p)
+        d.outlet_nodes = _p(keep["outlet_nodes"], capi._i64p)
+        d.outlet_normals = _p(keep["outlet_normals"], capi._f64p)
+        d.n_wall = len(keep["wall"])
+        d.wall = _p(keep["wall"], capi._i64p)
+        d.n_nearwall = self.n_nearwall
+        d.nearwall = _p(keep["nearwall"], capi._i64p)
+        d.nearwall_normals = _p(keep["nearwall_normal"], capi._f64p)
+        d.tau, d.dt, d.spacing = float(tau), float(dt), float(spacing)
+        h = ctypes.c_void_p()
+        capi.check(L.lbm_create(ctypes.byref(d), ctypes.byref(h)), None)
+        self._h = h
+        self._keep = keep
+        self.tau, self.dt, self.spacing = float(tau), float(dt), float(spacing)
+
+    # ---- lifecycle
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.lib().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, code):
+        return capi.check(code, self._h)
+
+    # ---- driving
+    def set_stream(self, stream_ptr):
+        self._check(capi.lib().lbm_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def set_flow(self, pulsatile=False, cte_vel=0.0):
+        self._check(capi.lib().lbm_set_flow(
+            self._h, capi.FLOW_PULSATILE if pulsatile else capi.FLOW_CONSTANT, float(cte_vel)))
+
+    def set_inlet_profile(self, vel):
+        v = np.ascontiguousarray(vel, dtype=np.float64).reshape(self.n_inlet, 3)
+        self._check(capi.lib().lbm_set_inlet_profile(self._h, _p(v, capi._f64p)))
+
+    def set_outlet_density(self, rho):
+        self._check(capi.lib().lbm_set_outlet_density(self._h, float(rho)))
+
+    def step(self, n=1):
+        self._check(capi.lib().lbm_step(self._h, int(n)))
+
+    def step_timed(self, n):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(capi.lib().lbm_step_timed(self._h, int(n), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    # ---- results
+    def time(self):
+        s, r = ctypes.c_int64(), ctypes.c_double()
+        self._check(capi.lib().lbm_get_time(self._h, ctypes.byref(s), ctypes.byref(r)))
+        return s.value, r.value
+
+    def populations(self, out=None):
+        f = np.empty((self.n, self.q)) if out is None else out
+        self._check(capi.lib().lbm_get_populations(self._h, f.ctypes.data))
+        return f
+
+    def set_populations(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64).reshape(self.n, self.q)
+        self._check(capi.lib().lbm_set_populations(self._h, f.ctypes.data))
+
+    def macros(self):
+        rho, u = np.empty(self.n), np.empty((self.n, 3))
+        self._check(capi.lib().lbm_get_macros(self._h, rho.ctypes.data, u.ctypes.data))
+        return rho, u
+
+    def wss(self):
+        m = self.n_nearwall
+        w, a, am = np.empty(m), np.empty((m, 3)), np.empty(m)
+        self._check(capi.lib().lbm_get_wss(self._h, w.ctypes.data, a.ctypes.data, am.ctypes.data))
+        return w, a, am
+
+    def osi_tawss(self):
+        m = self.n_nearwall
+        o, t = np.empty(m), np.empty(m)
+        self._check(capi.lib().lbm_get_osi_tawss(self._h, o.ctypes.data, t.ctypes.data))
+        return o, t
+
+    def flags(self):
+        v = ctypes.c_uint32()
+        self._check(capi.lib().lbm_get_flags(self._h, ctypes.byref(v)))
+        return v.value
+
+    def info(self):
+        vals = [ctypes.c_int64() for _ in range(6)]
+        self._check(capi.lib().lbm_get_info(self._h, *[ctypes.byref(v) for v in vals]))
+        keys = ("n_nodes", "ld", "n_segments", "n_nearwall", "n_outlet_nodes", "device_bytes")
+        return {k: v.value for k, v in zip(keys, vals)}
+
+
+class Simulation:
+    """The reference's Simulation (Simulation.h:54-90) on the engine.
+
+    params: dict with FlowType ("Constant" or "Pulsatile"), CteVel, MaxIter,
+    tau, dt and spacing — the SimulationParameters fields the loop uses.
+    ``on_output(iter, sim)`` is called where the reference calls WriteOutput
+    for constant flow (every IterToWrite steps, Simulation.cpp:596-603)."""
+
+    PERIOD = 0.9
+    PULSATILE_END = 2.7
+
+    def __init__(self, topo, params, storage="f64", on_output=None, device=0):
+        self.params = dict(params)
+        self.engine = Engine(topo, tau=params["tau"], dt=params.get("dt", 1e-5),
+                             spacing=params.get("spacing", 1.0), storage=storage,
+                             bc="reference", device=device)
+        self.pulsatile = params.get("FlowType", "Constant") == "Pulsatile"
+        self.engine.set_flow(self.pulsatile, params.get("CteVel", 0.0))
+        self.on_output = on_output
+
+    def Iterate(self):
+        p = self.params
+        if not self.pulsatile:
+            total = int(p["MaxIter"])
+            every = int(p.get("IterToWrite", 0) or 0)
+            done = 0
+            while done < total:
+                # next output point: iter > 0 and iter % IterToWrite == 0, after
+                # the step with that index (iter counts from 0)
+                chunk = total - done
+                if every and self.on_output:
+                    nxt = ((done // every) + 1) * every
+                    if nxt < total:
+                        chunk = nxt + 1 - done
+                self.engine.step(chunk)
+                done += chunk
+                it = done - 1
+                if every and self.on_output and it > 0 and it % every == 0:
+                    self.on_output(it, self)
+        else:
+            t, n = 0.0, 0
+            while t <= self.PULSATILE_END:
+                t += float(p["dt"])
+                n += 1
+            self.engine.step(n)

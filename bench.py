@@ -55,11 +55,11 @@ def build_workload(name):
     if name == "tortuous8":
         r = G.fluid_fraction_radius(0.08, BOX)
         topo = G.tortuous_vessel(radius=r, box=BOX)
-        desc = "tortuous stenosed vessel, 512x512x1024 box, ~8% fluid (radius %.1f lu)" % r
-    elif name == "tortuous20":
-        r = 20.0
+        desc = "tortuous stenosed vessel, 512x512x1024 box, ~8%% fluid (radius %.1f lu)" % r
+    elif name.startswith("tortuousR"):
+        r = float(name[len("tortuousR"):])
         topo = G.tortuous_vessel(radius=r, box=BOX)
-        desc = "tortuous stenosed vessel, 512x512x1024 box, radius 20 lu"
+        desc = "tortuous stenosed vessel, 512x512x1024 box, radius %g lu" % r
     elif name == "pipe":
         r = 16.0
         topo = G.straight_pipe(radius=r, length=136, box=(40, 40, 136))

@@ -96,3 +96,21 @@ def test_pulsatile_step_count_matches_loop_rule():
             t += dt
             n += 1
         assert orc.pulsatile_step_count(dt) == n
+
+
+def test_oracle_matches_reference_pipe_2000_steps():
+    """The R=16, L=128 pipe on the reference grid (102,555 nodes), 2000 steps:
+    sampled populations and moments, every near-wall WSS value and the
+    whole-field checksums equal the reference's."""
+    d = load(os.path.join(GOLDEN, "pipe16_2000.npz"))
+    o = orc.Oracle(d)
+    o.run(2000, cte_vel=float(d["meta_d"][4]))
+    s = d["sample"]
+    same(o.f[s], d["final__f_sample"], "f sample")
+    same(o.rho[s], d["final__rho_sample"], "rho sample")
+    same(o.u[s], d["final__u_sample"], "u sample")
+    same(o.wss, d["final__wss"], "wss")
+    same(o.acc, d["final__acc"], "acc")
+    same(o.accmag, d["final__accmag"], "accmag")
+    for k, a in (("f", o.f), ("rho", o.rho), ("u", o.u), ("feq", o.feq)):
+        same(np.array([a.sum(), np.abs(a).sum(), (a * a).sum()]), d["final__%s_sum" % k], k + " sums")

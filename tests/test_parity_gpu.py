@@ -122,3 +122,31 @@ def test_set_populations_roundtrip_and_continue():
     b.step(5)
     # b has no WSS history, but the flow fields must continue identically
     same(b.populations(), a.populations(), "continued state")
+
+
+def test_pipe_2000_steps_against_reference():
+    """The R=16, L=128 pipe the reference ran for 2000 steps (102,555 nodes):
+    FP64 equals the reference bit for bit on the sampled populations and
+    moments, every WSS value and the whole-field sums; FP32 stays within 1e-5."""
+    d = load(os.path.join(GOLDEN, "pipe16_2000.npz"))
+    s = d["sample"]
+    e = engine_for(d, "f64")
+    e.step(2000)
+    f = e.populations()
+    rho, u = e.macros()
+    w, acc, accm = e.wss()
+    same(f[s], d["final__f_sample"], "f sample")
+    same(rho[s], d["final__rho_sample"], "rho sample")
+    same(u[s], d["final__u_sample"], "u sample")
+    same(w, d["final__wss"], "wss")
+    same(acc, d["final__acc"], "acc")
+    same(accm, d["final__accmag"], "accmag")
+    same(np.array([f.sum(), np.abs(f).sum(), (f * f).sum()]), d["final__f_sum"], "f sums")
+    e32 = engine_for(d, "f32")
+    e32.step(2000)
+    assert rel(e32.populations()[s], d["final__f_sample"]) <= FP32_RTOL
+    rho32, u32 = e32.macros()
+    assert rel(u32[s], d["final__u_sample"]) <= FP32_RTOL
+    w32, acc32, _ = e32.wss()
+    assert rel(w32, d["final__wss"]) <= FP32_RTOL
+    assert rel(acc32, d["final__acc"]) <= FP32_RTOL

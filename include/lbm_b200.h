@@ -120,6 +120,14 @@ int lbm_set_outlet_density(lbm_engine* e, double rho);
  * below synchronise. */
 int lbm_step(lbm_engine* e, int64_t n_steps);
 
+/* Observation policy (default 1). With 1, the last two steps of every
+ * lbm_step call also store the state the getters read (populations, density
+ * and velocity); with 0 they do not, which saves that traffic when a caller
+ * steps many times between outputs (the reference reads state only at its
+ * output steps, Simulation.cpp:575-603). Population and moment getters fail
+ * with LBM_ERR_STATE after unobserved steps; WSS getters are always valid. */
+int lbm_set_observation(lbm_engine* e, int32_t enabled);
+
 /* Steps taken so far, and the flow clock (total_runtime). */
 int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime);
 

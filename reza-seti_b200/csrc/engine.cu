@@ -37,6 +37,7 @@ struct Topo {
     long long ld = 0;
     int nblocks = 0;
     int nseg = 0;
+    int max_block_segs = 1;
     std::vector<int> perm;   // internal -> caller
     std::vector<int> iperm;  // caller -> internal
     std::vector<uint64_t> meta;
@@ -161,6 +162,7 @@ std::string build_topology(const lbm_desc& d, Topo& t) {
         t.meta[i] = mask | ((uint64_t)kind[i] << M::KIND_SHIFT) | (rel << M::SEG_SHIFT);
     }
     t.seg_base[t.nblocks] = t.nseg;
+    for (int b = 0; b < t.nblocks; ++b) t.max_block_segs = std::max(t.max_block_segs, t.seg_base[b + 1] - t.seg_base[b]);
 
     auto node_of = [&](int64_t caller, int want_kind, const char* what, std::string& err) -> int {
         if (caller < 0 || caller >= n) {
@@ -221,7 +223,9 @@ std::string build_topology(const lbm_desc& d, Topo& t) {
             src_of[i] = src;
             t.aux[i] = (int)t.out_node.size();
             t.out_node.push_back(i);
-            t.out_src.push_back(src);
+            // a source that is an inlet node is encoded -(src + 2): the
+            // boundary pass applies its Zou-He update before copying
+            t.out_src.push_back(src >= 0 && kind[src] == KIND_INLET ? -(src + 2) : src);
             for (int c = 0; c < 3; ++c) t.out_nrm.push_back((float)nr[c]);
         }
     }
@@ -232,11 +236,17 @@ std::string build_topology(const lbm_desc& d, Topo& t) {
     for (int64_t k = 0; k < d.n_wall; ++k)
         if (node_of(d.wall[k], KIND_WALL, "wall", err) < 0) return err;
 
-    // near-wall nodes keep the caller's list order
+    // near-wall nodes keep the caller's list order; like the reference's
+    // nextToTheWall set (Subdomain.cpp:475-493) they are plain fluid nodes,
+    // each listed once
     if (d.n_nearwall < 0 || (d.n_nearwall > 0 && (!d.nearwall || !d.nearwall_normals))) return "bad near-wall list";
     for (int64_t k = 0; k < d.n_nearwall; ++k) {
-        if (d.nearwall[k] < 0 || d.nearwall[k] >= n) return "near-wall index out of range";
-        t.nw_node.push_back(t.iperm[d.nearwall[k]]);
+        const int i = node_of(d.nearwall[k], KIND_FLUID, "near-wall", err);
+        if (i < 0) return err;
+        if ((t.meta[i] >> M::NW_SHIFT) & 1) return "node listed twice in the near-wall list";
+        t.meta[i] |= 1ull << M::NW_SHIFT;
+        t.aux[i] = (int)k;
+        t.nw_node.push_back(i);
         for (int c = 0; c < 3; ++c) t.nw_normal.push_back(d.nearwall_normals[3 * k + c]);
     }
     return "";
@@ -285,7 +295,10 @@ struct lbm_engine {
     int64_t step = 0;
     double runtime = 0.0;
     int phase = 1;
-    int macro_buf = 0;
+    bool observe = true;       // lbm_set_observation
+    int64_t mom_step[2] = {-1, -1};  // step whose collision-input moments each obs_mom buffer holds
+    int64_t pop_step = -1;           // step whose post-boundary populations obs_pop holds
+    bool wss_pending = false;  // a step kernel handed near-wall populations not yet reduced to WSS
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     size_t bytes = 0;
@@ -302,6 +315,7 @@ struct lbm_engine {
     int* nw_node = nullptr;
     double* nw_normal = nullptr;
     double* nw_mom = nullptr;
+    void* nw_s = nullptr;
     double* wss = nullptr;
     double* acc = nullptr;
     double* accmag = nullptr;
@@ -367,6 +381,7 @@ StepArgs<S, Q> step_args(lbm_engine* e, double vel, float scale, double* mom) {
     a.meta = (const typename Meta<Q>::T*)e->meta;
     a.seg_base = e->seg_base;
     a.seg_delta = e->seg_delta;
+    a.seg_smem_bytes = e->t.max_block_segs * Q * (int)sizeof(int);
     a.aux = e->aux;
     a.omega = (C)e->omega;
     for (int c = 0; c < 3; ++c) {
@@ -380,6 +395,8 @@ StepArgs<S, Q> step_args(lbm_engine* e, double vel, float scale, double* mom) {
     a.in_scale = scale;
     a.out_nrm = e->out_nrm;
     a.out_rho = e->out_rho;
+    a.nw_s = (C*)e->nw_s;
+    a.n_nw = e->nw();
     a.obs_pop = e->obs_pop;
     a.obs_mom = mom;
     a.flags = e->flags;
@@ -387,7 +404,7 @@ StepArgs<S, Q> step_args(lbm_engine* e, double vel, float scale, double* mom) {
 }
 
 template <class S, int Q>
-BoundaryArgs<S, Q> boundary_args(lbm_engine* e, double vel) {
+BoundaryArgs<S, Q> boundary_args(lbm_engine* e, double vel, bool with_wss, bool with_outlets) {
     using C = typename Store<S>::C;
     BoundaryArgs<S, Q> b{};
     b.pop = (const S*)e->pop;
@@ -395,15 +412,16 @@ BoundaryArgs<S, Q> boundary_args(lbm_engine* e, double vel) {
     b.meta = (const typename Meta<Q>::T*)e->meta;
     b.seg_base = e->seg_base;
     b.seg_delta = e->seg_delta;
+    b.n_wss = with_wss ? e->nw() : 0;
     b.n_nw = e->nw();
-    b.nw_node = e->nw_node;
+    b.nw_s = (const C*)e->nw_s;
     b.nw_normal = e->nw_normal;
     b.nw_mom = e->nw_mom;
     b.wss = e->wss;
     b.acc = e->acc;
     b.accmag = e->accmag;
     b.wss_c = e->wss_c;
-    b.n_out = e->bc == LBM_BC_REFERENCE ? e->nout() : 0;
+    b.n_out = (with_outlets && e->bc == LBM_BC_REFERENCE) ? e->nout() : 0;
     b.out_src = e->out_src;
     b.out_buf = (C*)e->out_buf;
     for (int c = 0; c < 3; ++c) b.inlet_normal[c] = e->inlet_normal[c];
@@ -427,7 +445,10 @@ int init_from_obs(lbm_engine* e) {
                                              e->nw_mom, e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "near-wall moments");
     e->phase = 1;
-    e->macro_buf = mb;
+    e->wss_pending = false;
+    e->mom_step[mb] = e->step;
+    e->mom_step[1 - mb] = -1;
+    e->pop_step = e->step;
     return 0;
 }
 
@@ -437,12 +458,13 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
     if (t_step) *t_step = 0;
     if (t_bnd) *t_bnd = 0;
     const bool timed = t_step || t_bnd;
-    // timed runs: events ev[2i] before the pre-pass of step i, ev[2i+1]
-    // before its stream+collide kernel, ev[2n] after the last step; read once
-    // at the end so timing adds no host round trip between steps
+    // timed runs: events ev[2i] before the boundary pass of step i, ev[2i+1]
+    // before its stream+collide kernel, ev[2n] after the last step, ev[2n+1]
+    // after the last step's wall-shear pass; read once at the end so timing
+    // adds no host round trip between steps
     if (timed) {
         if (n_steps > (1 << 20)) return e->fail(LBM_ERR_ARGUMENT, "too many timed steps in one call");
-        while ((int64_t)e->evpool.size() < 2 * n_steps + 1) {
+        while ((int64_t)e->evpool.size() < 2 * n_steps + 2) {
             cudaEvent_t ev;
             cudaError_t ce = cudaEventCreate(&ev);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "event");
@@ -455,15 +477,16 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
         const double vel = pulsatile ? pulsatile_velocity(e->runtime, 0.9) : e->cte_vel;
         const float scale = e->bc == LBM_BC_REFERENCE ? 0.f : (float)(pulsatile ? vel : 1.0);
         int obs = 0;
-        if (i >= n_steps - 2) obs |= 2;
-        if (i == n_steps - 1) obs |= 1;
+        if (e->observe && i >= n_steps - 2) obs |= 2;
+        if (e->observe && i == n_steps - 1) obs |= 1;
         double* mom = e->obs_mom[t % 2];
         const int phase = e->phase;
         int rc = dispatch(e, [&](auto tag) {
             using S = typename decltype(tag)::St;
             constexpr int Q = decltype(tag)::q;
             if (timed) cudaEventRecord(e->evpool[2 * i], e->stream);
-            cudaError_t ce = launch_boundary<S, Q>(boundary_args<S, Q>(e, vel), phase, e->stream);
+            cudaError_t ce =
+                launch_boundary<S, Q>(boundary_args<S, Q>(e, vel, e->wss_pending, true), phase, e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "boundary kernel");
             if (timed) cudaEventRecord(e->evpool[2 * i + 1], e->stream);
             ce = launch_step<S, Q>(step_args<S, Q>(e, vel, scale, mom), phase, e->bc, obs, e->stream);
@@ -471,14 +494,28 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
             return 0;
         });
         if (rc) return rc;
+        if (obs & 2) e->mom_step[t % 2] = t;
+        if (obs & 1) e->pop_step = t;
+        e->wss_pending = e->nw() > 0;
         e->phase ^= 1;
         e->step = t;
         if (pulsatile) e->runtime += e->dt;
     }
-    e->macro_buf = (int)((e->step - 1) % 2);
+    // wall shear stress of the last step
+    if (timed) cudaEventRecord(e->evpool[2 * n_steps], e->stream);
+    if (e->wss_pending) {
+        int rc = dispatch(e, [&](auto tag) {
+            using S = typename decltype(tag)::St;
+            constexpr int Q = decltype(tag)::q;
+            cudaError_t ce = launch_boundary<S, Q>(boundary_args<S, Q>(e, 0.0, true, false), e->phase, e->stream);
+            return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "wall shear kernel");
+        });
+        if (rc) return rc;
+        e->wss_pending = false;
+    }
     if (timed) {
-        cudaEventRecord(e->evpool[2 * n_steps], e->stream);
-        cudaError_t ce = cudaEventSynchronize(e->evpool[2 * n_steps]);
+        cudaEventRecord(e->evpool[2 * n_steps + 1], e->stream);
+        cudaError_t ce = cudaEventSynchronize(e->evpool[2 * n_steps + 1]);
         if (ce != cudaSuccess) return e->cuda_fail(ce, "timed steps");
         double ms_step = 0, ms_bnd = 0;
         for (int64_t i = 0; i < n_steps; ++i) {
@@ -488,6 +525,9 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
             ms_bnd += a;
             ms_step += b;
         }
+        float last = 0;
+        cudaEventElapsedTime(&last, e->evpool[2 * n_steps], e->evpool[2 * n_steps + 1]);
+        ms_bnd += last;
         if (t_step) *t_step = ms_step;
         if (t_bnd) *t_bnd = ms_bnd;
     }
@@ -606,6 +646,9 @@ int create(const lbm_desc* d, lbm_engine** out) {
     if ((ce = e->upload(&e->nw_node, t.nw_node)) != cudaSuccess) return bail(ce, "near-wall");
     if ((ce = e->upload(&e->nw_normal, t.nw_normal)) != cudaSuccess) return bail(ce, "near-wall");
     if ((ce = e->alloc(&e->nw_mom, (size_t)4 * std::max(1, e->nw()))) != cudaSuccess) return bail(ce, "near-wall");
+    char* nws = nullptr;
+    if ((ce = e->alloc(&nws, (size_t)e->Q * std::max(1, e->nw()) * celem)) != cudaSuccess) return bail(ce, "near-wall");
+    e->nw_s = nws;
     if ((ce = e->alloc(&e->wss, (size_t)e->nw())) != cudaSuccess) return bail(ce, "wss");
     if ((ce = e->alloc(&e->acc, (size_t)3 * e->nw())) != cudaSuccess) return bail(ce, "wss");
     if ((ce = e->alloc(&e->accmag, (size_t)e->nw())) != cudaSuccess) return bail(ce, "wss");
@@ -696,6 +739,12 @@ int lbm_set_outlet_density(lbm_engine* e, double rho) {
     return 0;
 }
 
+int lbm_set_observation(lbm_engine* e, int32_t enabled) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    e->observe = enabled != 0;
+    return 0;
+}
+
 int lbm_step(lbm_engine* e, int64_t n_steps) {
     if (!e) return LBM_ERR_ARGUMENT;
     cudaSetDevice(e->device);
@@ -721,6 +770,7 @@ int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime) {
 
 int lbm_get_populations(lbm_engine* e, double* f) {
     if (!e || !f) return LBM_ERR_ARGUMENT;
+    if (e->pop_step != e->step) return e->fail(LBM_ERR_STATE, "populations of the last step were not observed");
     cudaSetDevice(e->device);
     if (int rc = ensure_staging(e)) return rc;
     cudaError_t ce = launch_pop_to_caller(e->obs_pop, e->perm, e->t.n, e->Q, e->t.ld, e->staging, e->stream);
@@ -749,7 +799,15 @@ int lbm_get_macros(lbm_engine* e, double* rho, double* u) {
     const int n = e->t.n;
     double* r = e->staging;
     double* uu = e->staging + n;
-    cudaError_t ce = launch_mom_to_caller(e->obs_mom[e->macro_buf], e->perm, n, e->t.ld, r, uu, e->stream);
+    // the moments the last step's collision used (those of the previous
+    // step's state); right after initialisation, those of the initial state
+    int b = (int)((e->step + 1) % 2);
+    if (e->step == 0 || e->mom_step[b] != e->step - 1) {
+        b = (int)(e->step % 2);
+        if (e->mom_step[b] != e->step || e->pop_step != e->step)
+            return e->fail(LBM_ERR_STATE, "moments of the last step were not observed");
+    }
+    cudaError_t ce = launch_mom_to_caller(e->obs_mom[b], e->perm, n, e->t.ld, r, uu, e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "reorder");
     if (rho && (ce = cudaMemcpyAsync(rho, r, sizeof(double) * n, cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess)
         return e->cuda_fail(ce, "download");

@@ -43,6 +43,7 @@ template <>
 struct Store<double> {
     using C = double;
     static constexpr bool SHIFTED = false;
+    static constexpr int MIN_BLOCKS = 1;  // resident 256-thread blocks per SM the step kernel targets
     __device__ static C get(const double* p) { return *p; }
     __device__ static void put(double* p, C v) { *p = v; }
 };
@@ -50,6 +51,7 @@ template <>
 struct Store<float> {
     using C = float;
     static constexpr bool SHIFTED = true;
+    static constexpr int MIN_BLOCKS = 4;
     __device__ static C get(const float* p) { return *p; }
     __device__ static void put(float* p, C v) { *p = v; }
 };
@@ -57,6 +59,7 @@ template <>
 struct Store<__half> {
     using C = float;
     static constexpr bool SHIFTED = true;
+    static constexpr int MIN_BLOCKS = 4;
     __device__ static C get(const __half* p) { return __half2float(*p); }
     __device__ static void put(__half* p, C v) { *p = __float2half_rn(v); }
 };
@@ -64,6 +67,7 @@ template <>
 struct Store<__nv_bfloat16> {
     using C = float;
     static constexpr bool SHIFTED = true;
+    static constexpr int MIN_BLOCKS = 4;
     __device__ static C get(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     __device__ static void put(__nv_bfloat16* p, C v) { *p = __float2bfloat16_rn(v); }
 };
@@ -86,7 +90,8 @@ struct StepArgs {
     const MT* meta;
     const int* seg_base;   // [blocks] first segment of each block
     const int* seg_delta;  // [segments][Q] neighbour index offsets
-    const int* aux;        // [n] index into the inlet / outlet tables (boundary kinds)
+    int seg_smem_bytes;    // shared memory for the largest block's segment rows
+    const int* aux;        // [n] index into the inlet / outlet / near-wall tables
     C omega;               // 1 / tau
     // reference-mode inlet: one normal and one velocity for all inlet nodes
     double inlet_normal[3];
@@ -101,6 +106,10 @@ struct StepArgs {
     double in_normal[3];   // outward inlet normal
     const float* out_nrm;  // [n_out][3] outward normal of each outlet node's outlet
     double out_rho;        // outlet density
+    // near-wall nodes: their arriving populations, [Q][n_nw], for the wall
+    // shear stress computed by the next boundary pass (aux[n] is the index)
+    C* nw_s;
+    int n_nw;
     // observation (written only by observing launches)
     double* obs_pop;       // [Q][ld] post-boundary populations f (natural layout)
     double* obs_mom;       // [4][ld] rho, ux, uy, uz
@@ -116,18 +125,20 @@ struct BoundaryArgs {
     const MT* meta;
     const int* seg_base;
     const int* seg_delta;
-    // near-wall nodes
+    // wall shear stress of the previous step's near-wall nodes (n_wss = 0
+    // when there is none pending)
+    int n_wss;
     int n_nw;
-    const int* nw_node;
+    const C* nw_s;            // [Q][n_nw] arriving populations of the previous step
     const double* nw_normal;  // [n_nw][3]
-    double* nw_mom;           // [n_nw][4] moments of the previous step (rho or rho-1, u)
+    double* nw_mom;           // [n_nw][4] moments that step's f_eq used (rho or rho-1, u)
     double* wss;              // [n_nw]
     double* acc;              // [n_nw][3]
     double* accmag;           // [n_nw]
     double wss_c;             // 1060 dt^2 / (spacing^2 1e-6)
-    // outlet sources
+    // outlet sources, one thread per (outlet node, direction)
     int n_out;
-    const int* out_src;       // [n_out] source node or -1
+    const int* out_src;       // [n_out] source node or -1; ~src for a source that is an inlet node
     C* out_buf;               // [n_out][Q]
     double inlet_normal[3];
     double inlet_vel;
@@ -154,7 +165,7 @@ __device__ __forceinline__ void gather(const S* __restrict__ pop, long long ld, 
             idx = (long long)q * ld + n;
         } else {
             const int oq = L::opp(q);
-            idx = ((m >> oq) & 1) ? (long long)oq * ld + (n + __ldg(sd + oq)) : (long long)q * ld + n;
+            idx = ((m >> oq) & 1) ? (long long)oq * ld + (n + sd[oq]) : (long long)q * ld + n;
         }
         s[q] = Store<S>::get(pop + idx);
     }
@@ -394,20 +405,101 @@ __device__ __forceinline__ void shear_traction(const C fne[Q], const double nrm_
     }
 }
 
+// Wall shear stress of near-wall node k from its arriving populations s and
+// the moments its previous collision used (the f_eq the reference keeps in
+// m_eqdistributions), accumulated in FP64 (Simulation.cpp:767-799).
+template <class S, int Q>
+__device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
+    using C = typename Store<S>::C;
+    using L = Lat<Q>;
+    C s[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s[q] = a.nw_s[(long long)q * a.n_nw + k];
+    double* mom = a.nw_mom + 4 * (long long)k;
+    const double* nd = a.nw_normal + 3 * (long long)k;
+    double tau[3];
+    if constexpr (sizeof(C) == 8) {
+        // FP64: the reference's own triple loop, operand order kept
+        C fne[Q];
+        const double u[3] = {mom[1], mom[2], mom[3]};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) fne[q] = s[q] - feq_ref<Q>(q, mom[0], u);
+        shear_traction<C, Q>(fne, nd, a.wss_c, tau);
+    } else {
+        // FP32: the same traction through the non-equilibrium stress tensor,
+        // Pi_ab = sum_q fne_q c_qa c_qb:  sum_q fne_q (c.n)(c_a - (c.n) n_a)
+        // = (Pi n)_a - (n.Pi.n) n_a
+        const float u[3] = {(float)mom[1], (float)mom[2], (float)mom[3]};
+        const float drho = (float)mom[0];
+        float P[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // xx yy zz xy xz yz
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (q == L::REST) continue;
+            const float fne = s[q] - deq_shifted<Q>(q, drho, u);
+            const int x = L::cx(q), y = L::cy(q), z = L::cz(q);
+            if (x) P[0] += fne;
+            if (y) P[1] += fne;
+            if (z) P[2] += fne;
+            if (x && y) P[3] += x * y > 0 ? fne : -fne;
+            if (x && z) P[4] += x * z > 0 ? fne : -fne;
+            if (y && z) P[5] += y * z > 0 ? fne : -fne;
+        }
+        const float n0 = (float)nd[0], n1 = (float)nd[1], n2 = (float)nd[2];
+        const float pn0 = P[0] * n0 + P[3] * n1 + P[4] * n2;
+        const float pn1 = P[3] * n0 + P[1] * n1 + P[5] * n2;
+        const float pn2 = P[4] * n0 + P[5] * n1 + P[2] * n2;
+        const float t = pn0 * n0 + pn1 * n1 + pn2 * n2;
+        tau[0] = a.wss_c * (double)(pn0 - t * n0);
+        tau[1] = a.wss_c * (double)(pn1 - t * n1);
+        tau[2] = a.wss_c * (double)(pn2 - t * n2);
+    }
+    const double w = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
+    a.wss[k] = w;
+    a.acc[3 * (long long)k] += tau[0];
+    a.acc[3 * (long long)k + 1] += tau[1];
+    a.acc[3 * (long long)k + 2] += tau[2];
+    a.accmag[k] += w;
+    // moments of these populations: the f_eq of the next step's WSS (the
+    // same arithmetic as that step's collision of this node)
+    C m0, u[3];
+    if constexpr (sizeof(C) == 8) {
+        double rho;
+        moments_ref<Q>(s, false, rho, u);
+        m0 = rho;
+    } else {
+        moments_shifted<Q>(s, false, m0, u);
+    }
+    mom[0] = (double)m0;
+    mom[1] = (double)u[0];
+    mom[2] = (double)u[1];
+    mom[3] = (double)u[2];
+}
+
 // ---------------------------------------------------------------- kernels ---
 // One AA step over all nodes. BC selects reference or physics boundaries;
 // OBS writes the post-boundary populations and/or moments for the host.
 template <class S, int Q, int PHASE, int BC, int OBS>
-__global__ void __launch_bounds__(BLOCK_NODES) step_kernel(StepArgs<S, Q> a) {
+__global__ void __launch_bounds__(BLOCK_NODES, Store<S>::MIN_BLOCKS) step_kernel(StepArgs<S, Q> a) {
     using L = Lat<Q>;
     using C = typename Store<S>::C;
     using MT = typename Meta<Q>::T;
+    extern __shared__ int seg_smem[];
     const int n = blockIdx.x * BLOCK_NODES + threadIdx.x;
-    if (n >= a.n) return;
-    const MT m = a.meta[n];
-    const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    const bool live = n < a.n;
+    const MT m = live ? a.meta[n] : MT(0);
     const int* sd = nullptr;
-    if (PHASE == 1) sd = seg_row<Q>(a.seg_base, a.seg_delta, n, m);
+    if (PHASE == 1) {
+        // the block's segment offsets, staged once in shared memory: the
+        // neighbour addresses then depend on one global load (meta) only
+        const int s0 = __ldg(a.seg_base + blockIdx.x);
+        const int cnt = (__ldg(a.seg_base + blockIdx.x + 1) - s0) * Q;
+        const int* src = a.seg_delta + (long long)s0 * Q;
+        for (int i = threadIdx.x; i < cnt; i += BLOCK_NODES) seg_smem[i] = __ldg(src + i);
+        __syncthreads();
+        sd = seg_smem + Q * (int)(m >> Meta<Q>::SEG_SHIFT);
+    }
+    if (!live) return;
+    const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
 
     C s[Q];
     gather<S, Q, PHASE>(a.pop, a.ld, n, m, sd, s);
@@ -426,7 +518,7 @@ __global__ void __launch_bounds__(BLOCK_NODES) step_kernel(StepArgs<S, Q> a) {
             if constexpr (Q == 19) zou_he<C>(s, a.inlet_normal, a.inlet_vel);
         } else if (kind == KIND_OUTLET) {
             const int k = a.aux[n];
-            if (a.out_src[k] >= 0) {
+            if (a.out_src[k] != -1) {
 #pragma unroll
                 for (int q = 0; q < Q; ++q) s[q] = a.out_buf[(long long)k * Q + q];
             }
@@ -439,6 +531,14 @@ __global__ void __launch_bounds__(BLOCK_NODES) step_kernel(StepArgs<S, Q> a) {
 #pragma unroll
         for (int q = 0; q < Q; ++q)
             a.obs_pop[(long long)q * a.ld + n] = Store<S>::SHIFTED ? (double)s[q] + L::w(q) : (double)s[q];
+    }
+
+    // near-wall nodes hand their arriving populations to the boundary pass
+    // that computes this step's wall shear stress
+    if ((m >> Meta<Q>::NW_SHIFT) & 1) {
+        const int k = a.aux[n];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) a.nw_s[(long long)q * a.n_nw + k] = s[q];
     }
 
     C c[Q], m0, u[3];
@@ -507,7 +607,7 @@ __global__ void __launch_bounds__(BLOCK_NODES) step_kernel(StepArgs<S, Q> a) {
             if (q == L::REST) {
                 Store<S>::put(a.pop + (long long)q * a.ld + n, c[q]);
             } else {
-                if ((m >> q) & 1) Store<S>::put(a.pop + (long long)q * a.ld + (n + __ldg(sd + q)), c[q]);
+                if ((m >> q) & 1) Store<S>::put(a.pop + (long long)q * a.ld + (n + sd[q]), c[q]);
                 const int oq = L::opp(q);
                 // slot (n, oq) is free when the node n - c_oq = n + c_q is missing
                 if (!((m >> q) & 1)) Store<S>::put(a.pop + (long long)oq * a.ld + n, back[q]);
@@ -553,70 +653,48 @@ __global__ void __launch_bounds__(BLOCK_NODES) init_kernel(StepArgs<S, Q> a) {
     }
 }
 
-// Boundary pre-pass of one reference-mode step, before the step kernel of the
-// same phase: wall shear stress of near-wall nodes from the arriving
-// populations and the previous step's moments, and the source populations of
-// every outlet node (post-streaming, post-inlet values of the node the
-// reference's in-order copy sweep ends up reading).
+// Boundary pass, launched before the step kernel of each step:
+//  * items [0, n_wss): wall shear stress of the previous step's near-wall
+//    nodes, from the populations that step's kernel handed over;
+//  * then one item per (outlet node, direction): the source population of
+//    the outlet copy (post-streaming, post-inlet value of the node the
+//    reference's in-order copy sweep ends up reading), gathered before the
+//    step kernel overwrites it. A source that is itself an inlet node needs
+//    its Zou-He update first, so one thread does that whole node.
 template <class S, int Q, int PHASE>
 __global__ void boundary_kernel(BoundaryArgs<S, Q> a) {
     using C = typename Store<S>::C;
     using MT = typename Meta<Q>::T;
     using L = Lat<Q>;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < a.n_nw) {
-        const int n = a.nw_node[i];
-        const MT m = a.meta[n];
-        const int* sd = PHASE == 1 ? seg_row<Q>(a.seg_base, a.seg_delta, n, m) : nullptr;
-        C s[Q];
-        gather<S, Q, PHASE>(a.pop, a.ld, n, m, sd, s);
-        const double* mom = a.nw_mom + 4 * (long long)i;
-        C fne[Q];
-        if constexpr (sizeof(C) == 8) {
-            const double u[3] = {mom[1], mom[2], mom[3]};
-#pragma unroll
-            for (int q = 0; q < Q; ++q) fne[q] = s[q] - feq_ref<Q>(q, mom[0], u);
-        } else {
-            const float u[3] = {(float)mom[1], (float)mom[2], (float)mom[3]};
-#pragma unroll
-            for (int q = 0; q < Q; ++q) fne[q] = s[q] - deq_shifted<Q>(q, (float)mom[0], u);
-        }
-        double tau[3];
-        shear_traction<C, Q>(fne, a.nw_normal + 3 * (long long)i, a.wss_c, tau);
-        const double w = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
-        a.wss[i] = w;
-        a.acc[3 * (long long)i] += tau[0];
-        a.acc[3 * (long long)i + 1] += tau[1];
-        a.acc[3 * (long long)i + 2] += tau[2];
-        a.accmag[i] += w;
-        // moments of this step's collision input, for the next step's f_eq
-        C m0, u[3];
-        if constexpr (sizeof(C) == 8) {
-            double rho;
-            moments_ref<Q>(s, false, rho, u);
-            m0 = rho;
-        } else {
-            moments_shifted<Q>(s, false, m0, u);
-        }
-        double* mo = a.nw_mom + 4 * (long long)i;
-        mo[0] = (double)m0;
-        mo[1] = (double)u[0];
-        mo[2] = (double)u[1];
-        mo[3] = (double)u[2];
-    } else if (i < a.n_nw + a.n_out) {
-        const int k = i - a.n_nw;
-        const int n = a.out_src[k];
-        if (n < 0) return;
-        const MT m = a.meta[n];
-        const int* sd = PHASE == 1 ? seg_row<Q>(a.seg_base, a.seg_delta, n, m) : nullptr;
-        C s[Q];
-        gather<S, Q, PHASE>(a.pop, a.ld, n, m, sd, s);
-        if constexpr (Q == 19) {
-            if ((int)((m >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET) zou_he<C>(s, a.inlet_normal, a.inlet_vel);
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) a.out_buf[(long long)k * Q + q] = s[q];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.n_wss) {
+        wall_shear<S, Q>(a, (int)i);
+        return;
     }
+    const long long j = i - a.n_wss;
+    if (j >= (long long)a.n_out * Q) return;
+    const int k = (int)(j / Q), q = (int)(j % Q);
+    const int src = a.out_src[k];
+    if (src == -1) return;
+    if (src <= -2) {
+        if (q != 0) return;
+        const int n = -(src + 2);
+        const MT m = a.meta[n];
+        const int* sd = PHASE == 1 ? seg_row<Q>(a.seg_base, a.seg_delta, n, m) : nullptr;
+        C s[Q];
+        gather<S, Q, PHASE>(a.pop, a.ld, n, m, sd, s);
+        if constexpr (Q == 19) zou_he<C>(s, a.inlet_normal, a.inlet_vel);
+#pragma unroll
+        for (int d = 0; d < Q; ++d) a.out_buf[(long long)k * Q + d] = s[d];
+        return;
+    }
+    const MT m = a.meta[src];
+    long long idx = (long long)q * a.ld + src;
+    if (PHASE == 1 && q != L::REST) {
+        const int oq = L::opp(q);
+        if ((m >> oq) & 1) idx = (long long)oq * a.ld + (src + seg_row<Q>(a.seg_base, a.seg_delta, src, m)[oq]);
+    }
+    a.out_buf[(long long)k * Q + q] = Store<S>::get(a.pop + idx);
 }
 
 }  // namespace lbm

@@ -71,17 +71,19 @@ struct Lat<27> {
 };
 
 // Per-node metadata word: bit q (q < Q) set when the neighbour in direction q
-// exists (the rest direction's bit is always set); two bits of node kind; the
-// remaining high bits hold the node's segment index relative to its block's
-// first segment. A segment is a run of consecutive nodes (in the compact
-// x-major, z-fastest order) whose neighbours in every direction sit at the
-// same index offset; the offsets are stored once per segment, so a node costs
-// one metadata word instead of a Q-entry neighbour table.
+// exists (the rest direction's bit is always set); two bits of node kind; one
+// bit marking a near-wall (wall-shear-stress) node; the remaining high bits
+// hold the node's segment index relative to its block's first segment. A
+// segment is a run of consecutive nodes (in the compact x-major, z-fastest
+// order) whose neighbours in every direction sit at the same index offset;
+// the offsets are stored once per segment, so a node costs one metadata word
+// instead of a Q-entry neighbour table.
 template <int Q>
 struct Meta {
     using T = typename std::conditional<(Q <= 19), uint32_t, uint64_t>::type;
     static constexpr int KIND_SHIFT = Q;
-    static constexpr int SEG_SHIFT = Q + 2;
+    static constexpr int NW_SHIFT = Q + 2;
+    static constexpr int SEG_SHIFT = Q + 3;
     static constexpr int SEG_BITS = (int)sizeof(T) * 8 - SEG_SHIFT;
     __host__ __device__ static constexpr T mask_all() { return (T(1) << Q) - 1; }
 };

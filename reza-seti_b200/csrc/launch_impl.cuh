@@ -8,11 +8,12 @@ namespace lbm {
 
 template <class S, int Q, int PHASE, int BC>
 static cudaError_t step_obs(const StepArgs<S, Q>& a, int obs, dim3 g, cudaStream_t st) {
+    const int smem = PHASE == 1 ? a.seg_smem_bytes : 0;
     switch (obs) {
-        case 0: step_kernel<S, Q, PHASE, BC, 0><<<g, BLOCK_NODES, 0, st>>>(a); break;
-        case 1: step_kernel<S, Q, PHASE, BC, 1><<<g, BLOCK_NODES, 0, st>>>(a); break;
-        case 2: step_kernel<S, Q, PHASE, BC, 2><<<g, BLOCK_NODES, 0, st>>>(a); break;
-        default: step_kernel<S, Q, PHASE, BC, 3><<<g, BLOCK_NODES, 0, st>>>(a); break;
+        case 0: step_kernel<S, Q, PHASE, BC, 0><<<g, BLOCK_NODES, smem, st>>>(a); break;
+        case 1: step_kernel<S, Q, PHASE, BC, 1><<<g, BLOCK_NODES, smem, st>>>(a); break;
+        case 2: step_kernel<S, Q, PHASE, BC, 2><<<g, BLOCK_NODES, smem, st>>>(a); break;
+        default: step_kernel<S, Q, PHASE, BC, 3><<<g, BLOCK_NODES, smem, st>>>(a); break;
     }
     return cudaGetLastError();
 }
@@ -41,10 +42,10 @@ cudaError_t launch_init(const StepArgs<S, Q>& a, int bc, cudaStream_t st) {
 
 template <class S, int Q>
 cudaError_t launch_boundary(const BoundaryArgs<S, Q>& a, int phase, cudaStream_t st) {
-    const int items = a.n_nw + a.n_out;
+    const long long items = (long long)a.n_wss + (long long)a.n_out * Q;
     if (items == 0) return cudaSuccess;
     const int tpb = 128;
-    const dim3 g((items + tpb - 1) / tpb);
+    const dim3 g((unsigned)((items + tpb - 1) / tpb));
     if (phase) boundary_kernel<S, Q, 1><<<g, tpb, 0, st>>>(a);
     else boundary_kernel<S, Q, 0><<<g, tpb, 0, st>>>(a);
     return cudaGetLastError();

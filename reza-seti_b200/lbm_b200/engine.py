@@ -117,6 +117,9 @@ class Engine:
     def set_outlet_density(self, rho):
         self._check(capi.lib().lbm_set_outlet_density(self._h, float(rho)))
 
+    def set_observation(self, enabled):
+        self._check(capi.lib().lbm_set_observation(self._h, 1 if enabled else 0))
+
     def step(self, n=1):
         self._check(capi.lib().lbm_step(self._h, int(n)))
 

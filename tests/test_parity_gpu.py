@@ -150,3 +150,25 @@ def test_pipe_2000_steps_against_reference():
     w32, acc32, _ = e32.wss()
     assert rel(w32, d["final__wss"]) <= FP32_RTOL
     assert rel(acc32, d["final__acc"]) <= FP32_RTOL
+
+
+def test_observation_switch():
+    """Unobserved steps keep WSS valid but refuse population and moment reads;
+    the next observed call restores them, equal to an always-observed run."""
+    d = load(os.path.join(GOLDEN, "cyl_z.npz"))
+    a = engine_for(d)
+    b = engine_for(d)
+    b.set_observation(False)
+    a.step(7)
+    b.step(7)
+    same(b.wss()[0], a.wss()[0], "wss of unobserved steps")
+    with pytest.raises(capi.LbmError) as ei:
+        b.populations()
+    assert ei.value.code == capi.LBM_ERR_STATE
+    with pytest.raises(capi.LbmError):
+        b.macros()
+    b.set_observation(True)
+    a.step(3)
+    b.step(3)
+    same(b.populations(), a.populations(), "populations after observed call")
+    same(b.macros()[1], a.macros()[1], "velocity after observed call")

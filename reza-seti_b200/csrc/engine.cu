@@ -25,6 +25,7 @@
 
 #include "lbm_b200.h"
 #include "launch.h"
+#include "reduce.cuh"
 
 using namespace lbm;
 
@@ -47,6 +48,8 @@ struct Topo {
     std::vector<int> in_node;   // internal index per caller inlet entry
     std::vector<int> out_node;  // internal index per outlet-table entry
     std::vector<int> out_src;   // source node (internal) or -1
+    std::vector<long long> out_off;   // [n_outlets + 1] outlet k's entries of out_node
+    std::vector<double> out_normal;   // [n_outlets][3]
     std::vector<float> out_nrm; // [n_out][3]
     std::vector<int> nw_node;
     std::vector<double> nw_normal;
@@ -211,6 +214,9 @@ std::string build_topology(const lbm_desc& d, Topo& t) {
         else any = false;
         const int64_t b = d.outlet_offsets[o], e = d.outlet_offsets[o + 1];
         if (b < 0 || e < b) return "bad outlet offsets";
+        if (o == 0) t.out_off.push_back(0);
+        t.out_off.push_back((long long)(t.out_node.size() + (e - b)));
+        for (int c = 0; c < 3; ++c) t.out_normal.push_back(nr[c]);
         for (int64_t k = b; k < e; ++k) {
             const int i = node_of(d.outlet_nodes[k], KIND_OUTLET, "outlet", err);
             if (i < 0) return err;
@@ -324,6 +330,9 @@ struct lbm_engine {
     unsigned* flags = nullptr;
     float* in_vel = nullptr;
     int* perm = nullptr;
+    long long* flux_nodes = nullptr;  // internal indices: the inlet list, then the outlet lists
+    double* flux_partials = nullptr;
+    double* flux_out = nullptr;
     double* staging = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> evpool;
@@ -659,6 +668,15 @@ int create(const lbm_desc* d, lbm_engine** out) {
     std::vector<float> zero_in((size_t)3 * std::max(1, e->nin()), 0.f);
     if ((ce = e->upload(&e->in_vel, zero_in)) != cudaSuccess) return bail(ce, "inlet profile");
     if ((ce = e->upload(&e->perm, t.perm)) != cudaSuccess) return bail(ce, "permutation");
+    {
+        std::vector<long long> fl;
+        for (int i : t.in_node) fl.push_back(i);
+        for (int i : t.out_node) fl.push_back(i);
+        if ((ce = e->upload(&e->flux_nodes, fl)) != cudaSuccess) return bail(ce, "flux lists");
+        const size_t blocks = (fl.size() + FLUX_THREADS - 1) / FLUX_THREADS + 1;
+        if ((ce = e->alloc(&e->flux_partials, blocks)) != cudaSuccess) return bail(ce, "flux scratch");
+        if ((ce = e->alloc(&e->flux_out, (size_t)d->n_outlets + 1)) != cudaSuccess) return bail(ce, "flux scratch");
+    }
 
     cudaMemsetAsync(e->wss, 0, sizeof(double) * std::max(1, e->nw()), e->stream);
     cudaMemsetAsync(e->acc, 0, sizeof(double) * 3 * std::max(1, e->nw()), e->stream);
@@ -842,6 +860,29 @@ int lbm_get_osi_tawss(lbm_engine* e, double* osi, double* tawss) {
         if (osi) osi[k] = 0.5 * (1.0 - (norm / accmag[k]));
         if (tawss) tawss[k] = ta * e->dt;
     }
+    return 0;
+}
+
+int lbm_get_flux(lbm_engine* e, double* inlet, double* outlets) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    if (e->pop_step != e->step) return e->fail(LBM_ERR_STATE, "populations of the last step were not observed");
+    cudaSetDevice(e->device);
+    const int n_out = (int)e->t.out_normal.size() / 3;
+    cudaError_t ce = launch_flux(e->Q, e->obs_pop, 1, e->t.ld, e->flux_nodes, e->nin(), e->inlet_normal,
+                                 e->flux_partials, e->flux_out, e->stream);
+    for (int o = 0; o < n_out && ce == cudaSuccess; ++o) {
+        const long long b = e->t.out_off[o], n = e->t.out_off[o + 1] - b;
+        ce = launch_flux(e->Q, e->obs_pop, 1, e->t.ld, e->flux_nodes + e->nin() + b, n, &e->t.out_normal[3 * o],
+                         e->flux_partials, e->flux_out + 1 + o, e->stream);
+    }
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "flux kernels");
+    std::vector<double> h((size_t)n_out + 1);
+    ce = cudaMemcpyAsync(h.data(), e->flux_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "download");
+    if (int rc = sync(e)) return rc;
+    if (inlet) *inlet = h[0];
+    if (outlets)
+        for (int o = 0; o < n_out; ++o) outlets[o] = h[1 + o];
     return 0;
 }
 

@@ -68,6 +68,7 @@ SIGNATURES = {
     "lbm_get_macros": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),
     "lbm_get_wss": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "lbm_get_osi_tawss": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),
+    "lbm_get_flux": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),
     "lbm_get_flags": (ctypes.c_int, [_E, ctypes.POINTER(ctypes.c_uint32)]),
     "lbm_step_timed": (ctypes.c_int, [_E, ctypes.c_int64, _f64p, _f64p]),
     "lbm_get_info": (ctypes.c_int, [_E, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),

@@ -58,6 +58,7 @@ class Engine:
         self.n = len(keep["kind"])
         self.n_nearwall = len(keep["nearwall"])
         self.n_inlet = len(keep["inlet"])
+        self.n_outlets = len(outs)
         d = capi.LbmDesc()
         d.lattice = lattice
         d.storage = capi.STORAGE[storage]
@@ -159,6 +160,13 @@ class Engine:
         o, t = np.empty(m), np.empty(m)
         self._check(capi.lib().lbm_get_osi_tawss(self._h, o.ctypes.data, t.ctypes.data))
         return o, t
+
+    def flux(self):
+        """(inlet flux, [outlet fluxes]) of the last observed state, FP64."""
+        inl = np.empty(1)
+        outs = np.empty(max(1, self.n_outlets))
+        self._check(capi.lib().lbm_get_flux(self._h, inl.ctypes.data, outs.ctypes.data))
+        return float(inl[0]), outs[: self.n_outlets].copy()
 
     def flags(self):
         v = ctypes.c_uint32()

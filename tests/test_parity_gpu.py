@@ -172,3 +172,20 @@ def test_observation_switch():
     b.step(3)
     same(b.populations(), a.populations(), "populations after observed call")
     same(b.macros()[1], a.macros()[1], "velocity after observed call")
+
+
+def test_boundary_mass_flux_fp64():
+    """Inlet and outlet mass flux (FP64 device reduction) equal the sum over
+    each list of (sum_q c_q f_q) . normal computed on the host."""
+    d = load(os.path.join(GOLDEN, "outlet_chain.npz"))
+    e = engine_for(d)
+    e.step(12)
+    f = e.populations()
+    c = orc.directions().astype(np.float64)
+    inl, outs = e.flux()
+    want_in = float(np.sum(f[d["inlet"]] @ (c @ d["inlet_normal"])))
+    assert abs(inl - want_in) <= 1e-12 * max(1.0, abs(want_in))
+    for k, got in enumerate(outs):
+        want = float(np.sum(f[d["outlet_%d" % k]] @ (c @ d["outlet_normal_%d" % k])))
+        assert abs(got - want) <= 1e-12 * max(1.0, abs(want))
+    assert inl < 0  # flow enters through the inlet against its outward normal

@@ -1,11 +1,11 @@
 """Benchmark of the B200 LBM engine's time step (MLUPS and HBM roofline).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload tortuous8|tortuous20|pipe] [--storage f32|f16|bf16|f64]
+                    [--workload tortuous8|tortuousR<radius>|pipe] [--storage f32|f16|bf16|f64]
 
 Workload (default): the tortuous stenosed vessel in a 512 x 512 x 1024 box —
 sinusoidal centerline (amplitude 30 lu, wavelength 200 lu), Gaussian 50 %-area
-stenosis at mid-length, D3Q19, tau 0.52, plug inlet 0.05 lu — at the stated
+stenosis at mid-length, D3Q19, tau 0.52, plug inlet at Re = 300 — at the stated
 ~8 % fluid fraction of the box (radius from fluid_fraction_radius). The
 vessel's own radius 20 lu gives ~0.6 % of the box; that variant is timed too
 and reported under "variants". Inputs are synthetic and seeded (none needed:
@@ -46,7 +46,15 @@ sys.path.insert(0, os.path.join(ROOT, "reza-seti_b200"))
 METRIC = "MLUPS"
 BYTES_PER_POP = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}
 TAU = 0.52
-INLET_VEL = 0.05
+REYNOLDS = 300.0
+
+
+def inlet_velocity(radius):
+    """Plug inlet velocity (lattice units) giving Re = u D / nu = 300 for the
+    vessel diameter, with nu = (tau - 1/2) / 3 — the precision config's Re."""
+    return REYNOLDS * (TAU - 0.5) / 3.0 / (2.0 * radius)
+
+
 BOX = (512, 512, 1024)
 
 
@@ -161,10 +169,10 @@ def dist_setup(n_gpus):
     return world, rank, local, pg
 
 
-def time_engine(topo, storage, steps, warmup, device, torch):
+def time_engine(topo, storage, steps, warmup, device, torch, vel):
     from lbm_b200 import Engine
     eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device)
-    eng.set_flow(False, INLET_VEL)
+    eng.set_flow(False, vel)
     # timed steps store no observable state (the C ABI's observation switch);
     # the end-to-end measurement below turns it back on
     eng.set_observation(False)
@@ -188,6 +196,7 @@ def run_gpu(args):
     device = local
     torch.cuda.set_device(device)
     topo, desc, radius = build_workload(args.workload)
+    vel = inlet_velocity(radius)
     n = len(topo["kind"])
     storage = args.storage
     S = BYTES_PER_POP[storage]
@@ -198,7 +207,7 @@ def run_gpu(args):
         dist.barrier()
     torch.cuda.synchronize(device)
     with ClockSampler(device) as clk:
-        eng, total_ms, ms_step, ms_bnd = time_engine(topo, storage, args.steps, args.warmup, device, torch)
+        eng, total_ms, ms_step, ms_bnd = time_engine(topo, storage, args.steps, args.warmup, device, torch, vel)
     torch.cuda.synchronize(device)
     if dist:
         t = torch.tensor([total_ms], device="cuda")
@@ -232,7 +241,7 @@ def run_gpu(args):
 
     variants = {}
     if rank == 0 and not args.no_variants:
-        variants = run_variants(args, topo, n, torch, device)
+        variants = run_variants(args, topo, n, torch, device, vel)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -248,7 +257,7 @@ def run_gpu(args):
             "data": "synthetic (analytic vessel geometry, f = w initial state)",
             "config": {"workload": desc, "lattice": "D3Q19", "fluid_nodes": n,
                        "box_cells": BOX[0] * BOX[1] * BOX[2] if args.workload.startswith("tortuous") else None,
-                       "tau": TAU, "inlet_velocity": INLET_VEL, "storage": storage,
+                       "tau": TAU, "inlet_velocity": round(vel, 6), "reynolds": REYNOLDS, "storage": storage,
                        "bc_mode": "reference", "segments": info["n_segments"],
                        "near_wall_nodes": info["n_nearwall"],
                        "l2": "state larger than L2 (no flush)",
@@ -284,13 +293,13 @@ def end_to_end(eng, n, Q, steps, torch):
             "seconds": round(dt, 4)}
 
 
-def run_variants(args, topo, n, torch, device):
+def run_variants(args, topo, n, torch, device, vel):
     out = {}
     steps = max(10, args.steps // 2)
     for storage in ("f16", "bf16", "f64"):
         if storage == args.storage:
             continue
-        eng, total_ms, ms_step, _ = time_engine(topo, storage, steps, args.warmup, device, torch)
+        eng, total_ms, ms_step, _ = time_engine(topo, storage, steps, args.warmup, device, torch, vel)
         S = BYTES_PER_POP[storage]
         out[storage] = {"MLUPS": round(n * steps / (total_ms / 1e3) / 1e6, 1),
                         "step_kernel_GBs": round(2 * 19 * S * n / (ms_step / steps / 1e3) / 1e9, 1)}
@@ -299,7 +308,8 @@ def run_variants(args, topo, n, torch, device):
         from lbm_b200 import geometry as G
         t20 = G.tortuous_vessel(radius=20.0, box=BOX)
         n20 = len(t20["kind"])
-        eng, total_ms, ms_step, _ = time_engine(t20, "f32", steps, args.warmup, device, torch)
+        eng, total_ms, ms_step, _ = time_engine(t20, "f32", steps, args.warmup, device, torch,
+                                                inlet_velocity(20.0))
         out["radius20_f32"] = {"fluid_nodes": n20,
                                "MLUPS": round(n20 * steps / (total_ms / 1e3) / 1e6, 1)}
         eng.close()
@@ -346,7 +356,8 @@ def cpu_reference(args, sample_only=False, steps=None, procs=None):
     harness = os.path.join(ROOT, "oracle", "_ref", "refharness")
     if not os.path.exists(harness):
         return {"value": None, "unit": "MLUPS", "unavailable": "oracle/_ref/refharness not built"}
-    topo, desc, _ = build_workload(args.workload)
+    topo, desc, radius = build_workload(args.workload)
+    vel = inlet_velocity(radius)
     ncores = os.cpu_count() or 1
     procs = procs or (1 if sample_only else min(ncores, 32))
     steps = steps or (8 if sample_only else max(3, args.steps // 10))
@@ -356,7 +367,7 @@ def cpu_reference(args, sample_only=False, steps=None, procs=None):
     with open(cfg, "w") as fh:
         fh.write("parameters:\n\n  FlowType: \"Constant\"\n  time_resolution: 1e-05\n"
                  "  relaxation_factor: %r\n  grid_size: 0.5\n  CteVel: %r\n  MaxIter: %d\n"
-                 "  IterToWrite: 100000000\n\n" % (TAU, INLET_VEL, steps))
+                 "  IterToWrite: 100000000\n\n" % (TAU, vel, steps))
     runs = []
     nodes_total = 0
     for p in range(procs):
@@ -377,6 +388,7 @@ def cpu_reference(args, sample_only=False, steps=None, procs=None):
     slowest = max(r["seconds"] for r in results)
     value = sum(r["nodes"] for r in results) * steps / slowest / 1e6
     return {"value": round(value, 4), "unit": "MLUPS", "cores": procs, "kind": "reference",
+            "workload": desc, "inlet_velocity": round(vel, 6),
             "sample": "%d slab(s) of %d z-layers of the workload (%d nodes), %d steps each, "
                       "reference Simulation step methods, serial MPI build"
                       % (procs, layers, nodes_total, steps)}
@@ -396,8 +408,8 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (analytic vessel geometry, f = w initial state)",
-            "config": {"workload": build_workload(args.workload)[1], "lattice": "D3Q19",
-                       "tau": TAU, "inlet_velocity": INLET_VEL},
+            "config": {"workload": cpu.get("workload"), "lattice": "D3Q19", "tau": TAU,
+                       "inlet_velocity": cpu.get("inlet_velocity"), "reynolds": REYNOLDS},
             "cpu_baseline": cpu,
             "e2e": {"value": cpu["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},

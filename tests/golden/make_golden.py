@@ -92,13 +92,13 @@ def write_stl(path, tris):
 
 
 def write_config(path, *, flow="Constant", dt=1e-5, tau=0.8, grid_size=0.5, vel=0.05,
-                 max_iter=100, inlet, outlets):
+                 max_iter=100, iter_to_write=1000000, inlet, outlets):
     lines = ["parameters:", "", '  stl_file: "geom.stl"', '  FlowType: "%s"' % flow,
              "  time_resolution: %r" % dt, "  density: 1060", "  kinematic_viscosity: 3.5e-6",
              "  relaxation_factor: %r" % tau, "  grid_size: %r" % grid_size, "  pressure: 1",
              "  CteVel: %r" % vel, "  reynolds_number: 100",
              "  number_of_outlets: %d" % len(outlets), "  MaxIter: %d" % max_iter,
-             "  IterToWrite: 1000000", "  Systole: 0.15", "  Diastole: 0.9", "  period: 0.9",
+             "  IterToWrite: %d" % iter_to_write, "  Systole: 0.15", "  Diastole: 0.9", "  period: 0.9",
              "  NumCycle: 1", "", ""]
 
     def block(b):

@@ -161,6 +161,29 @@ int lbm_get_osi_tawss(lbm_engine* e, double* osi, double* tawss);
  * entries. Either may be NULL. */
 int lbm_get_flux(lbm_engine* e, double* inlet, double* outlets);
 
+/* Longest node list lbm_flux_noalloc accepts. */
+#define LBM_FLUX_NOALLOC_MAX_NODES 1048576
+
+/* Allocation-free mass flux. No counterpart in the reference. For callers
+ * that cannot allocate device memory: a framework that owns all device memory
+ * through its own pool and hands out only pointers into it, a process that may
+ * not allocate after start-up, or post-processing of populations held in
+ * another program's buffers without creating an engine (lbm_create allocates
+ * the whole lattice). Computes in FP64, on the device, the same quantity as
+ * lbm_get_flux: the sum over nodes[0 .. n_list) of (sum_q c_q f[node][q]) .
+ * normal, from populations f laid out [n_nodes][q] (q = 19 or 27, the
+ * reference's direction order). f, nodes and flux are device pointers; *flux
+ * receives the sum; normal is a host array. It allocates nothing: the block
+ * partial sums go to a fixed 32 KiB device array inside the library, so
+ * n_list may not exceed LBM_FLUX_NOALLOC_MAX_NODES (longer lists are rejected
+ * with LBM_ERR_ARGUMENT). Runs asynchronously on `stream` (a cudaStream_t, NULL
+ * for the default stream). The first call on a device looks up that array's
+ * device address; make it outside any stream capture. Every call on a device
+ * shares the array, so calls that overlap on the GPU race. List entries
+ * outside [0, n_nodes) contribute nothing. Errors: lbm_last_error(NULL). */
+int lbm_flux_noalloc(const double* f, int64_t n_nodes, int32_t q, const int64_t* nodes, int64_t n_list,
+                     const double normal[3], double* flux, void* stream);
+
 /* Device status bits since creation: 1 = a streamed population was exactly
  * zero (the reference would not have streamed it), 2 = non-finite density. */
 int lbm_get_flags(lbm_engine* e, uint32_t* flags);

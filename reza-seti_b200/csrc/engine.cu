@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "errors.h"
 #include "lbm_b200.h"
 #include "launch.h"
 #include "reduce.cuh"
@@ -910,5 +911,11 @@ int lbm_get_info(lbm_engine* e, int64_t* n_nodes, int64_t* ld, int64_t* n_segmen
 }
 
 const char* lbm_last_error(const lbm_engine* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
+
+}  // extern "C"
+
+void lbm::set_global_error(const std::string& msg) { g_create_error = msg; }
+
+extern "C" {
 
 }  // extern "C"

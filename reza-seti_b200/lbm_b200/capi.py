@@ -18,6 +18,7 @@ LBM_ERR_CUDA = -2
 LBM_ERR_NO_DEVICE = -3
 LBM_ERR_STATE = -4
 LBM_ERR_NUMERIC = -5
+FLUX_NOALLOC_MAX_NODES = 1048576  # LBM_FLUX_NOALLOC_MAX_NODES
 
 STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 BC_REFERENCE, BC_PHYSICS = 0, 1
@@ -69,6 +70,9 @@ SIGNATURES = {
     "lbm_get_wss": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "lbm_get_osi_tawss": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),
     "lbm_get_flux": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),
+    "lbm_flux_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
+                                        ctypes.c_int64, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
+                                        ctypes.c_void_p]),
     "lbm_get_flags": (ctypes.c_int, [_E, ctypes.POINTER(ctypes.c_uint32)]),
     "lbm_step_timed": (ctypes.c_int, [_E, ctypes.c_int64, _f64p, _f64p]),
     "lbm_get_info": (ctypes.c_int, [_E, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),

@@ -50,9 +50,20 @@ REYNOLDS = 300.0
 
 
 def inlet_velocity(radius):
-    """Plug inlet velocity (lattice units) giving Re = u D / nu = 300 for the
+    """Mean inlet velocity (lattice units) giving Re = u D / nu = 300 for the
     vessel diameter, with nu = (tau - 1/2) / 3 — the precision config's Re."""
     return REYNOLDS * (TAU - 0.5) / 3.0 / (2.0 * radius)
+
+
+def inlet_profile(topo, radius, mean):
+    """Parabolic inflow along +z with the given mean velocity over the inlet
+    disc (peak 2 x mean), centred on the inlet nodes."""
+    xy = topo["coords"][topo["inlet"]][:, :2].astype(np.float64)
+    c = xy.mean(axis=0)
+    r2 = ((xy - c) ** 2).sum(axis=1)
+    v = np.zeros((len(xy), 3))
+    v[:, 2] = np.maximum(0.0, 2.0 * mean * (1.0 - r2 / (radius * radius)))
+    return v
 
 
 BOX = (512, 512, 1024)
@@ -169,10 +180,12 @@ def dist_setup(n_gpus):
     return world, rank, local, pg
 
 
-def time_engine(topo, storage, steps, warmup, device, torch, vel):
+def time_engine(topo, storage, steps, warmup, device, torch, vel, bc="physics", radius=None):
     from lbm_b200 import Engine
-    eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device)
+    eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device, bc=bc)
     eng.set_flow(False, vel)
+    if bc == "physics":
+        eng.set_inlet_profile(inlet_profile(topo, radius, vel))
     # timed steps store no observable state (the C ABI's observation switch);
     # the end-to-end measurement below turns it back on
     eng.set_observation(False)
@@ -207,7 +220,8 @@ def run_gpu(args):
         dist.barrier()
     torch.cuda.synchronize(device)
     with ClockSampler(device) as clk:
-        eng, total_ms, ms_step, ms_bnd = time_engine(topo, storage, args.steps, args.warmup, device, torch, vel)
+        eng, total_ms, ms_step, ms_bnd = time_engine(topo, storage, args.steps, args.warmup, device, torch, vel,
+                                                     args.bc, radius)
     torch.cuda.synchronize(device)
     if dist:
         t = torch.tensor([total_ms], device="cuda")
@@ -241,7 +255,7 @@ def run_gpu(args):
 
     variants = {}
     if rank == 0 and not args.no_variants:
-        variants = run_variants(args, topo, n, torch, device, vel)
+        variants = run_variants(args, topo, n, torch, device, vel, radius)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -258,7 +272,7 @@ def run_gpu(args):
             "config": {"workload": desc, "lattice": "D3Q19", "fluid_nodes": n,
                        "box_cells": BOX[0] * BOX[1] * BOX[2] if args.workload.startswith("tortuous") else None,
                        "tau": TAU, "inlet_velocity": round(vel, 6), "reynolds": REYNOLDS, "storage": storage,
-                       "bc_mode": "reference", "segments": info["n_segments"],
+                       "bc_mode": args.bc, "segments": info["n_segments"],
                        "near_wall_nodes": info["n_nearwall"],
                        "l2": "state larger than L2 (no flush)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -293,13 +307,14 @@ def end_to_end(eng, n, Q, steps, torch):
             "seconds": round(dt, 4)}
 
 
-def run_variants(args, topo, n, torch, device, vel):
+def run_variants(args, topo, n, torch, device, vel, radius):
     out = {}
     steps = max(10, args.steps // 2)
     for storage in ("f16", "bf16", "f64"):
         if storage == args.storage:
             continue
-        eng, total_ms, ms_step, _ = time_engine(topo, storage, steps, args.warmup, device, torch, vel)
+        eng, total_ms, ms_step, _ = time_engine(topo, storage, steps, args.warmup, device, torch, vel,
+                                                args.bc, radius)
         S = BYTES_PER_POP[storage]
         out[storage] = {"MLUPS": round(n * steps / (total_ms / 1e3) / 1e6, 1),
                         "step_kernel_GBs": round(2 * 19 * S * n / (ms_step / steps / 1e3) / 1e9, 1)}
@@ -309,10 +324,16 @@ def run_variants(args, topo, n, torch, device, vel):
         t20 = G.tortuous_vessel(radius=20.0, box=BOX)
         n20 = len(t20["kind"])
         eng, total_ms, ms_step, _ = time_engine(t20, "f32", steps, args.warmup, device, torch,
-                                                inlet_velocity(20.0))
+                                                inlet_velocity(20.0), args.bc, 20.0)
         out["radius20_f32"] = {"fluid_nodes": n20,
                                "MLUPS": round(n20 * steps / (total_ms / 1e3) / 1e6, 1)}
         eng.close()
+    other = "reference" if args.bc == "physics" else "physics"
+    eng, total_ms, ms_step, _ = time_engine(topo, "f32", steps, args.warmup, device, torch, vel, other, radius)
+    out[other + "_bc_f32"] = {"MLUPS": round(n * steps / (total_ms / 1e3) / 1e6, 1),
+                              "step_kernel_GBs": round(2 * 19 * 4 * n / (ms_step / steps / 1e3) / 1e9, 1),
+                              "device_flags": eng.flags()}
+    eng.close()
     return out
 
 
@@ -425,6 +446,7 @@ def main():
     ap.add_argument("--impl", default="engine")
     ap.add_argument("--workload", default="tortuous8")
     ap.add_argument("--storage", default="f32")
+    ap.add_argument("--bc", default="physics", choices=["physics", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -89,8 +89,9 @@ typedef struct {
     double spacing;                /* Geometry::spacing (mm), for the WSS scale */
 } lbm_desc;
 
-/* Flow types of Simulation::Iterate (Simulation.cpp:549-562). */
-typedef enum { LBM_FLOW_CONSTANT = 0, LBM_FLOW_PULSATILE = 1 } lbm_flow;
+/* Flow types: the two of Simulation::Iterate (Simulation.cpp:549-562), and a
+ * harmonic waveform (lbm_set_waveform) for physics-mode inflow. */
+typedef enum { LBM_FLOW_CONSTANT = 0, LBM_FLOW_PULSATILE = 1, LBM_FLOW_HARMONIC = 2 } lbm_flow;
 
 /* Replaces Simulation(SubDomain&, SimulationParameters&) up to Iterate():
  * flattens the node graph to device arrays and sets f = w (Node::Initialize,
@@ -107,9 +108,19 @@ int lbm_set_stream(lbm_engine* e, void* stream);
  * advances by dt per pulsatile step. */
 int lbm_set_flow(lbm_engine* e, int32_t flow, double cte_vel);
 
-/* Physics mode: inlet velocity per inlet node [n_inlet][3] (lattice units),
- * multiplied each step by the waveform factor (1 for constant flow). */
+/* Physics mode: inlet velocity per inlet node [n_inlet][3] (lattice units,
+ * caller's inlet list order), multiplied each step by the waveform factor: 1
+ * for constant flow, the reference waveform value for pulsatile flow, the
+ * harmonic factor for harmonic flow. */
 int lbm_set_inlet_profile(lbm_engine* e, const double* velocity);
+
+/* Harmonic waveform (no counterpart in the reference, whose waveform is the
+ * fixed polynomial of pulsatile.h): factor(t) = 1 + sum_k amplitude[k]
+ * cos(2 pi (k+1) t / period_steps + phase[k]), t = index of the step (0 for
+ * the first). With LBM_FLOW_HARMONIC the reference-mode inlet velocity is
+ * cte_vel * factor and the physics-mode profile is scaled by factor. */
+int lbm_set_waveform(lbm_engine* e, double period_steps, int32_t n_harmonics, const double* amplitude,
+                     const double* phase);
 
 /* Physics mode: outlet density (default 1). */
 int lbm_set_outlet_density(lbm_engine* e, double rho);

@@ -306,6 +306,7 @@ struct lbm_engine {
     int64_t mom_step[2] = {-1, -1};  // step whose collision-input moments each obs_mom buffer holds
     int64_t pop_step = -1;           // step whose post-boundary populations obs_pop holds
     bool wss_pending = false;  // a step kernel handed near-wall populations not yet reduced to WSS
+    bool fresh = false;        // no step since the last initialisation
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     size_t bytes = 0;
@@ -329,7 +330,13 @@ struct lbm_engine {
     double* obs_pop = nullptr;
     double* obs_mom[2] = {nullptr, nullptr};
     unsigned* flags = nullptr;
-    float* in_vel = nullptr;
+    double* in_vel = nullptr;
+    int* in_node = nullptr;    // internal index per inlet-list entry
+    int* out_node = nullptr;   // internal index per outlet-table entry
+    double* io_u = nullptr;    // physics mode: outlet node velocities [n_out][3]
+    // harmonic waveform: factor 1 + sum_k amp_k cos(2 pi k t / period + phase_k), t in steps
+    double wave_period = 1.0;
+    std::vector<double> wave_amp, wave_phase;
     int* perm = nullptr;
     long long* flux_nodes = nullptr;  // internal indices: the inlet list, then the outlet lists
     double* flux_partials = nullptr;
@@ -382,7 +389,7 @@ int dispatch(lbm_engine* e, F&& f) {
 }
 
 template <class S, int Q>
-StepArgs<S, Q> step_args(lbm_engine* e, double vel, float scale, double* mom) {
+StepArgs<S, Q> step_args(lbm_engine* e, double vel, double* mom) {
     using C = typename Store<S>::C;
     StepArgs<S, Q> a{};
     a.pop = (S*)e->pop;
@@ -394,17 +401,11 @@ StepArgs<S, Q> step_args(lbm_engine* e, double vel, float scale, double* mom) {
     a.seg_smem_bytes = e->t.max_block_segs * Q * (int)sizeof(int);
     a.aux = e->aux;
     a.omega = (C)e->omega;
-    for (int c = 0; c < 3; ++c) {
-        a.inlet_normal[c] = e->inlet_normal[c];
-        a.in_normal[c] = e->inlet_normal[c];
-    }
+    for (int c = 0; c < 3; ++c) a.inlet_normal[c] = e->inlet_normal[c];
     a.inlet_vel = vel;
     a.out_src = e->out_src;
     a.out_buf = (const C*)e->out_buf;
-    a.in_vel = e->in_vel;
-    a.in_scale = scale;
-    a.out_nrm = e->out_nrm;
-    a.out_rho = e->out_rho;
+    a.io_u = e->io_u;
     a.nw_s = (C*)e->nw_s;
     a.n_nw = e->nw();
     a.obs_pop = e->obs_pop;
@@ -439,6 +440,52 @@ BoundaryArgs<S, Q> boundary_args(lbm_engine* e, double vel, bool with_wss, bool 
     return b;
 }
 
+template <class S, int Q>
+OpenArgs<S, Q> open_args(lbm_engine* e, double scale) {
+    OpenArgs<S, Q> o{};
+    o.pop = (S*)e->pop;
+    o.ld = e->t.ld;
+    o.meta = (const typename Meta<Q>::T*)e->meta;
+    o.n_in = e->nin();
+    o.in_node = e->in_node;
+    o.in_vel = e->in_vel;
+    o.in_scale = scale;
+    for (int c = 0; c < 3; ++c) o.in_normal[c] = e->inlet_normal[c];
+    o.n_out = e->nout();
+    o.out_node = e->out_node;
+    o.out_nrm = e->out_nrm;
+    o.io_u = e->io_u;
+    o.out_rho = e->out_rho;
+    return o;
+}
+
+// Inlet waveform factor of step k (0-based) whose flow clock reads runtime_k:
+// 1 for constant flow, the reference waveform value for pulsatile flow, the
+// harmonic factor for harmonic flow.
+double inlet_factor(const lbm_engine* e, int64_t k, double runtime_k) {
+    if (e->flow == LBM_FLOW_PULSATILE) return pulsatile_velocity(runtime_k, 0.9);
+    double f = 1.0;
+    if (e->flow == LBM_FLOW_HARMONIC) {
+        const double two_pi = 6.283185307179586;
+        for (size_t h = 0; h < e->wave_amp.size(); ++h)
+            f += e->wave_amp[h] * std::cos(two_pi * (double)(h + 1) * (double)k / e->wave_period + e->wave_phase[h]);
+    }
+    return f;
+}
+
+// Physics mode: corrects the open-boundary links of the store just issued,
+// which streams into step k.
+int open_pass(lbm_engine* e, int64_t k, double runtime_k) {
+    if (e->bc != LBM_BC_PHYSICS || e->nin() + e->nout() == 0) return 0;
+    const double scale = inlet_factor(e, k, runtime_k);
+    return dispatch(e, [&](auto tag) {
+        using S = typename decltype(tag)::St;
+        constexpr int Q = decltype(tag)::q;
+        cudaError_t ce = launch_open<S, Q>(open_args<S, Q>(e, scale), e->stream);
+        return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "open-boundary kernel");
+    });
+}
+
 // Collides the natural-layout state in obs_pop into the AA buffer and primes
 // the near-wall moments; the next step reads phase 1.
 int init_from_obs(lbm_engine* e) {
@@ -446,11 +493,12 @@ int init_from_obs(lbm_engine* e) {
     int rc = dispatch(e, [&](auto tag) {
         using S = typename decltype(tag)::St;
         constexpr int Q = decltype(tag)::q;
-        auto a = step_args<S, Q>(e, 0.0, 0.f, e->obs_mom[mb]);
+        auto a = step_args<S, Q>(e, 0.0, e->obs_mom[mb]);
         cudaError_t ce = launch_init<S, Q>(a, e->bc, e->stream);
         return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "init kernel");
     });
     if (rc) return rc;
+    if (int rc2 = open_pass(e, e->step, e->runtime)) return rc2;
     cudaError_t ce = launch_nearwall_moments(e->nw(), e->nw_node, e->obs_mom[mb], e->t.ld, e->shifted(),
                                              e->nw_mom, e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "near-wall moments");
@@ -459,6 +507,7 @@ int init_from_obs(lbm_engine* e) {
     e->mom_step[mb] = e->step;
     e->mom_step[1 - mb] = -1;
     e->pop_step = e->step;
+    e->fresh = true;
     return 0;
 }
 
@@ -484,8 +533,9 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
     for (int64_t i = 0; i < n_steps; ++i) {
         const int64_t t = e->step + 1;
         const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
-        const double vel = pulsatile ? pulsatile_velocity(e->runtime, 0.9) : e->cte_vel;
-        const float scale = e->bc == LBM_BC_REFERENCE ? 0.f : (float)(pulsatile ? vel : 1.0);
+        // reference-mode inlet velocity of this step (Simulation.cpp:558-562)
+        const double vel = pulsatile ? pulsatile_velocity(e->runtime, 0.9)
+                                     : e->cte_vel * inlet_factor(e, e->step, e->runtime);
         int obs = 0;
         if (e->observe && i >= n_steps - 2) obs |= 2;
         if (e->observe && i == n_steps - 1) obs |= 1;
@@ -499,17 +549,20 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
                 launch_boundary<S, Q>(boundary_args<S, Q>(e, vel, e->wss_pending, true), phase, e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "boundary kernel");
             if (timed) cudaEventRecord(e->evpool[2 * i + 1], e->stream);
-            ce = launch_step<S, Q>(step_args<S, Q>(e, vel, scale, mom), phase, e->bc, obs, e->stream);
+            ce = launch_step<S, Q>(step_args<S, Q>(e, vel, mom), phase, e->bc, obs, e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "step kernel");
             return 0;
         });
         if (rc) return rc;
+        // physics mode: this store streams into the next step
+        if (int rc2 = open_pass(e, e->step + 1, pulsatile ? e->runtime + e->dt : e->runtime)) return rc2;
         if (obs & 2) e->mom_step[t % 2] = t;
         if (obs & 1) e->pop_step = t;
         e->wss_pending = e->nw() > 0;
         e->phase ^= 1;
         e->step = t;
         if (pulsatile) e->runtime += e->dt;
+        e->fresh = false;
     }
     // wall shear stress of the last step
     if (timed) cudaEventRecord(e->evpool[2 * n_steps], e->stream);
@@ -666,8 +719,11 @@ int create(const lbm_desc* d, lbm_engine** out) {
     for (auto& m : e->obs_mom)
         if ((ce = e->alloc(&m, (size_t)4 * t.ld)) != cudaSuccess) return bail(ce, "observation buffer");
     if ((ce = e->alloc(&e->flags, 1)) != cudaSuccess) return bail(ce, "flags");
-    std::vector<float> zero_in((size_t)3 * std::max(1, e->nin()), 0.f);
+    std::vector<double> zero_in((size_t)3 * std::max(1, e->nin()), 0.0);
     if ((ce = e->upload(&e->in_vel, zero_in)) != cudaSuccess) return bail(ce, "inlet profile");
+    if ((ce = e->upload(&e->in_node, t.in_node)) != cudaSuccess) return bail(ce, "inlet list");
+    if ((ce = e->upload(&e->out_node, t.out_node)) != cudaSuccess) return bail(ce, "outlet list");
+    if ((ce = e->alloc(&e->io_u, (size_t)3 * std::max(1, e->nout()))) != cudaSuccess) return bail(ce, "outlet velocity");
     if ((ce = e->upload(&e->perm, t.perm)) != cudaSuccess) return bail(ce, "permutation");
     {
         std::vector<long long> fl;
@@ -733,29 +789,51 @@ int lbm_set_stream(lbm_engine* e, void* stream) {
     return 0;
 }
 
+// Physics mode applies the inlet and outlet conditions when it stores a step's
+// populations; a parameter set before the first step must reach the store of
+// the initialisation too, so that store is redone.
+static int reapply_initial_store(lbm_engine* e) {
+    if (e->bc != LBM_BC_PHYSICS || !e->fresh) return 0;
+    cudaSetDevice(e->device);
+    if (int rc = init_from_obs(e)) return rc;
+    return sync(e);
+}
+
+int lbm_set_waveform(lbm_engine* e, double period_steps, int32_t n_harmonics, const double* amplitude,
+                     const double* phase) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    if (!(period_steps > 0) || n_harmonics < 0 || (n_harmonics > 0 && (!amplitude || !phase)))
+        return e->fail(LBM_ERR_ARGUMENT, "bad waveform");
+    e->wave_period = period_steps;
+    e->wave_amp.assign(amplitude, amplitude + n_harmonics);
+    e->wave_phase.assign(phase, phase + n_harmonics);
+    return reapply_initial_store(e);
+}
+
 int lbm_set_flow(lbm_engine* e, int32_t flow, double cte_vel) {
     if (!e) return LBM_ERR_ARGUMENT;
-    if (flow != LBM_FLOW_CONSTANT && flow != LBM_FLOW_PULSATILE) return e->fail(LBM_ERR_ARGUMENT, "unknown flow type");
+    if (flow != LBM_FLOW_CONSTANT && flow != LBM_FLOW_PULSATILE && flow != LBM_FLOW_HARMONIC)
+        return e->fail(LBM_ERR_ARGUMENT, "unknown flow type");
     e->flow = flow;
     e->cte_vel = cte_vel;
-    return 0;
+    return reapply_initial_store(e);
 }
 
 int lbm_set_inlet_profile(lbm_engine* e, const double* velocity) {
     if (!e || !velocity) return LBM_ERR_ARGUMENT;
-    std::vector<float> v((size_t)3 * e->nin());
-    for (size_t i = 0; i < v.size(); ++i) v[i] = (float)velocity[i];
+    std::vector<double> v(velocity, velocity + (size_t)3 * e->nin());
     if (v.empty()) return 0;
     cudaSetDevice(e->device);
-    cudaError_t ce = cudaMemcpyAsync(e->in_vel, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream);
+    cudaError_t ce = cudaMemcpyAsync(e->in_vel, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "inlet profile");
-    return sync(e);
+    if (int rc = sync(e)) return rc;
+    return reapply_initial_store(e);
 }
 
 int lbm_set_outlet_density(lbm_engine* e, double rho) {
     if (!e) return LBM_ERR_ARGUMENT;
     e->out_rho = rho;
-    return 0;
+    return reapply_initial_store(e);
 }
 
 int lbm_set_observation(lbm_engine* e, int32_t enabled) {

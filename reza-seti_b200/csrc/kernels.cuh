@@ -100,12 +100,9 @@ struct StepArgs {
     // populations copied from its source (written by the pre-pass)
     const int* out_src;
     const C* out_buf;
-    // physics-mode boundaries
-    const float* in_vel;   // [n_in][3] inlet velocity profile (lattice units)
-    float in_scale;        // waveform factor of this step
-    double in_normal[3];   // outward inlet normal
-    const float* out_nrm;  // [n_out][3] outward normal of each outlet node's outlet
-    double out_rho;        // outlet density
+    // physics mode: velocity of each outlet node's collision, [n_out][3],
+    // for the open-boundary pass
+    double* io_u;
     // near-wall nodes: their arriving populations, [Q][n_nw], for the wall
     // shear stress computed by the next boundary pass (aux[n] is the index)
     C* nw_s;
@@ -554,43 +551,17 @@ __global__ void __launch_bounds__(BLOCK_NODES, Store<S>::MIN_BLOCKS) step_kernel
 
     // Values for links whose far end is missing: reference mode keeps the
     // node's own pre-collision value of the opposite direction; physics mode
-    // bounces the post-collision population back, corrected on inlet and
-    // outlet links.
+    // bounces the post-collision population back (the open-boundary pass then
+    // corrects inlet and outlet links, and needs the outlet node's velocity).
     C back[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        if constexpr (BC == BC_REFERENCE) {
-            back[q] = s[L::opp(q)];
-        } else {
-            C v = c[q];
-            if (kind == KIND_INLET || kind == KIND_OUTLET) {
-                double nrm[3];
-                if (kind == KIND_INLET) {
-                    nrm[0] = a.in_normal[0], nrm[1] = a.in_normal[1], nrm[2] = a.in_normal[2];
-                } else {
-                    const float* o = a.out_nrm + 3 * (long long)a.aux[n];
-                    nrm[0] = o[0], nrm[1] = o[1], nrm[2] = o[2];
-                }
-                const double cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
-                if (cn > 0.0) {
-                    if (kind == KIND_INLET) {
-                        const int k = a.aux[n];
-                        const C uw[3] = {C(a.in_vel[3 * k] * a.in_scale), C(a.in_vel[3 * k + 1] * a.in_scale),
-                                         C(a.in_vel[3 * k + 2] * a.in_scale)};
-                        const C cu = L::cx(q) * uw[0] + L::cy(q) * uw[1] + L::cz(q) * uw[2];
-                        v = c[q] - C(6.0 * L::w(q)) * cu;
-                    } else {
-                        const C cu = L::cx(q) * u[0] + L::cy(q) * u[1] + L::cz(q) * u[2];
-                        const C usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-                        const C eq = C(1) + C(4.5) * cu * cu - C(1.5) * usq;
-                        if constexpr (Store<S>::SHIFTED)
-                            v = -c[q] + C(2.0 * L::w(q)) * (C(a.out_rho) * eq - C(1));
-                        else
-                            v = -c[q] + C(2.0 * L::w(q) * a.out_rho) * eq;
-                    }
-                }
-            }
-            back[q] = v;
+    for (int q = 0; q < Q; ++q) back[q] = BC == BC_REFERENCE ? s[L::opp(q)] : c[q];
+    if constexpr (BC == BC_PHYSICS) {
+        if (kind == KIND_OUTLET) {
+            double* o = a.io_u + 3 * (long long)a.aux[n];
+            o[0] = (double)u[0];
+            o[1] = (double)u[1];
+            o[2] = (double)u[2];
         }
     }
 
@@ -644,12 +615,85 @@ __global__ void __launch_bounds__(BLOCK_NODES) init_kernel(StepArgs<S, Q> a) {
     a.obs_mom[a.ld + n] = (double)u[0];
     a.obs_mom[2 * a.ld + n] = (double)u[1];
     a.obs_mom[3 * a.ld + n] = (double)u[2];
+    if (BC == BC_PHYSICS && kind == KIND_OUTLET) {
+        double* o = a.io_u + 3 * (long long)a.aux[n];
+        o[0] = (double)u[0];
+        o[1] = (double)u[1];
+        o[2] = (double)u[2];
+    }
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const int oq = L::opp(q);
         C v = c[q];
         if (q != L::REST && !((m >> q) & 1)) v = BC == BC_REFERENCE ? s[oq] : c[q];
         Store<S>::put(a.pop + (long long)oq * a.ld + n, v);
+    }
+}
+
+// Open-boundary pass of physics mode, after every store (step or
+// initialisation). The store bounced back every population whose far node is
+// missing into slot (n, opp q); on inlet and outlet nodes the links that point
+// out through the open plane (c_q . n > 0) are corrected here:
+//   inlet  (velocity bounce-back): f <- f - 6 w_q (c_q . u_in)
+//   outlet (anti-bounce-back at rho_out): f <- -f + 2 w_q rho_out
+//          (1 + 4.5 (c_q . u)^2 - 1.5 u^2), u the node's collision velocity.
+// Items: inlet nodes, then outlet nodes.
+template <class S, int Q>
+struct OpenArgs {
+    S* pop;
+    long long ld;
+    const typename Meta<Q>::T* meta;
+    int n_in;
+    const int* in_node;     // [n_in]
+    const double* in_vel;   // [n_in][3] inlet velocity profile
+    double in_scale;        // waveform factor of the step the store streams into
+    double in_normal[3];    // outward inlet normal
+    int n_out;
+    const int* out_node;    // [n_out]
+    const float* out_nrm;   // [n_out][3] outward normal of each node's outlet
+    const double* io_u;     // [n_out][3] velocity of each outlet node
+    double out_rho;
+};
+
+template <class S, int Q>
+__global__ void open_boundary_kernel(OpenArgs<S, Q> a) {
+    using L = Lat<Q>;
+    using C = typename Store<S>::C;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_in + a.n_out) return;
+    const bool inlet = i < a.n_in;
+    const int k = inlet ? i : i - a.n_in;
+    const int n = inlet ? a.in_node[k] : a.out_node[k];
+    const typename Meta<Q>::T m = a.meta[n];
+    double nrm[3], uv[3];
+    if (inlet) {
+        for (int c = 0; c < 3; ++c) {
+            nrm[c] = a.in_normal[c];
+            uv[c] = a.in_vel[3 * (long long)k + c] * a.in_scale;
+        }
+    } else {
+        for (int c = 0; c < 3; ++c) {
+            nrm[c] = a.out_nrm[3 * (long long)k + c];
+            uv[c] = a.io_u[3 * (long long)k + c];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (q == L::REST || ((m >> q) & 1)) continue;
+        const double cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
+        if (!(cn > 0.0)) continue;
+        S* slot = a.pop + (long long)L::opp(q) * a.ld + n;
+        const double f = (double)Store<S>::get(slot);
+        const double cu = L::cx(q) * uv[0] + L::cy(q) * uv[1] + L::cz(q) * uv[2];
+        double v;
+        if (inlet) {
+            v = f - 6.0 * L::w(q) * cu;
+        } else {
+            const double eq = 1.0 + 4.5 * cu * cu - 1.5 * (uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
+            // stored deviations: -(w + d) + 2 w rho eq - w = -d + 2 w (rho eq - 1)
+            v = Store<S>::SHIFTED ? -f + 2.0 * L::w(q) * (a.out_rho * eq - 1.0) : -f + 2.0 * L::w(q) * a.out_rho * eq;
+        }
+        Store<S>::put(slot, (C)v);
     }
 }
 

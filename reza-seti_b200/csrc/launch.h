@@ -17,6 +17,9 @@ cudaError_t launch_init(const StepArgs<S, Q>& a, int bc, cudaStream_t st);
 template <class S, int Q>
 cudaError_t launch_boundary(const BoundaryArgs<S, Q>& a, int phase, cudaStream_t st);
 
+template <class S, int Q>
+cudaError_t launch_open(const OpenArgs<S, Q>& a, cudaStream_t st);
+
 // Fills natural-layout populations with the lattice weights (f = w).
 cudaError_t launch_fill_weights(double* obs_pop, long long ld, int n, int q, cudaStream_t st);
 

@@ -51,9 +51,18 @@ cudaError_t launch_boundary(const BoundaryArgs<S, Q>& a, int phase, cudaStream_t
     return cudaGetLastError();
 }
 
+template <class S, int Q>
+cudaError_t launch_open(const OpenArgs<S, Q>& a, cudaStream_t st) {
+    const int items = a.n_in + a.n_out;
+    if (items == 0) return cudaSuccess;
+    open_boundary_kernel<S, Q><<<(items + 127) / 128, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
 #define LBM_INSTANTIATE(S, Q)                                                                          \
     template cudaError_t launch_step<S, Q>(const StepArgs<S, Q>&, int, int, int, cudaStream_t);        \
     template cudaError_t launch_init<S, Q>(const StepArgs<S, Q>&, int, cudaStream_t);                  \
-    template cudaError_t launch_boundary<S, Q>(const BoundaryArgs<S, Q>&, int, cudaStream_t);
+    template cudaError_t launch_boundary<S, Q>(const BoundaryArgs<S, Q>&, int, cudaStream_t);          \
+    template cudaError_t launch_open<S, Q>(const OpenArgs<S, Q>&, cudaStream_t);
 
 }  // namespace lbm

@@ -22,7 +22,7 @@ FLUX_NOALLOC_MAX_NODES = 1048576  # LBM_FLUX_NOALLOC_MAX_NODES
 
 STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 BC_REFERENCE, BC_PHYSICS = 0, 1
-FLOW_CONSTANT, FLOW_PULSATILE = 0, 1
+FLOW_CONSTANT, FLOW_PULSATILE, FLOW_HARMONIC = 0, 1, 2
 FLAG_ZERO_SKIP, FLAG_NONFINITE = 1, 2
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -60,6 +60,7 @@ SIGNATURES = {
     "lbm_set_stream": (ctypes.c_int, [_E, ctypes.c_void_p]),
     "lbm_set_flow": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_double]),
     "lbm_set_inlet_profile": (ctypes.c_int, [_E, _f64p]),
+    "lbm_set_waveform": (ctypes.c_int, [_E, ctypes.c_double, ctypes.c_int32, _f64p, _f64p]),
     "lbm_set_outlet_density": (ctypes.c_int, [_E, ctypes.c_double]),
     "lbm_step": (ctypes.c_int, [_E, ctypes.c_int64]),
     "lbm_set_observation": (ctypes.c_int, [_E, ctypes.c_int32]),

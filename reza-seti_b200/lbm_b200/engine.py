@@ -107,9 +107,15 @@ class Engine:
     def set_stream(self, stream_ptr):
         self._check(capi.lib().lbm_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 
-    def set_flow(self, pulsatile=False, cte_vel=0.0):
-        self._check(capi.lib().lbm_set_flow(
-            self._h, capi.FLOW_PULSATILE if pulsatile else capi.FLOW_CONSTANT, float(cte_vel)))
+    def set_flow(self, pulsatile=False, cte_vel=0.0, harmonic=False):
+        kind = capi.FLOW_HARMONIC if harmonic else (capi.FLOW_PULSATILE if pulsatile else capi.FLOW_CONSTANT)
+        self._check(capi.lib().lbm_set_flow(self._h, kind, float(cte_vel)))
+
+    def set_waveform(self, period_steps, amplitude, phase):
+        a = np.ascontiguousarray(amplitude, dtype=np.float64)
+        p = np.ascontiguousarray(phase, dtype=np.float64)
+        self._check(capi.lib().lbm_set_waveform(self._h, float(period_steps), len(a), _p(a, capi._f64p),
+                                                _p(p, capi._f64p)))
 
     def set_inlet_profile(self, vel):
         v = np.ascontiguousarray(vel, dtype=np.float64).reshape(self.n_inlet, 3)

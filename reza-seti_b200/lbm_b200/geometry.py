@@ -216,5 +216,20 @@ def straight_pipe(radius=16.0, length=128, box=None, centre=None, stenosis=0.0, 
                              np.arange(Z, dtype=float), indexing="ij")
     p = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
     fluid = (field(p) < 0).reshape(box)
-    return classify(fluid, box, (0, 0, 0), inlet_z=0, outlet_z=Z - 1,
+    topo = classify(fluid, box, (0, 0, 0), inlet_z=0, outlet_z=Z - 1,
                     normal_fn=lambda pts: _normals_from_field(field, pts))
+    topo["axis_centre"] = np.array([cx, cy])
+    topo["radius"] = np.array([radius])
+    return topo
+
+
+def parabolic_inlet(topo, u_max, radius=None, centre=None):
+    """Poiseuille inlet profile along +z for the inlet nodes of a pipe:
+    u_z = u_max (1 - r^2 / R^2), zero outside R ([n_inlet, 3])."""
+    R = float(topo["radius"][0]) if radius is None else radius
+    cx, cy = topo["axis_centre"] if centre is None else centre
+    xy = topo["coords"][topo["inlet"]][:, :2].astype(np.float64)
+    r2 = (xy[:, 0] - cx) ** 2 + (xy[:, 1] - cy) ** 2
+    v = np.zeros((len(xy), 3))
+    v[:, 2] = np.maximum(0.0, u_max * (1.0 - r2 / (R * R)))
+    return v

@@ -209,6 +209,48 @@ int lbm_step_timed(lbm_engine* e, int64_t n_steps, double* step_kernel_ms, doubl
 int lbm_get_info(lbm_engine* e, int64_t* n_nodes, int64_t* ld, int64_t* n_segments, int64_t* n_nearwall,
                  int64_t* n_outlet_nodes, int64_t* device_bytes);
 
+/* Adjoint sensitivities of a time-averaged wall-shear objective. No
+ * counterpart in the reference (whose WSS, Simulation.cpp:767-799, is only
+ * evaluated). Physics mode only (D3Q19 or D3Q27).
+ *
+ * Starting from the engine's current populations (those of its last step,
+ * which must have been observed), the run integrates n_steps physics-mode
+ * steps with its own copy of the state, leaving the engine unchanged:
+ * halfway bounce-back walls, the anti-bounce-back outlet at the engine's
+ * outlet density, and an inlet whose speed along -inlet_normal at inlet node
+ * i is v_i = sum_j coeffs[j] basis[j][i] (the engine's own inlet profile is
+ * not used), times the engine's waveform factor of each step. Objective:
+ *   J = (1/T) sum_{t=1..T} sum_{k in target} |tau_k^t|^2,
+ * tau_k^t the wall-shear traction vector of near-wall entry k at step t, with
+ * the definition and scale of lbm_get_wss. With gradient = 1 it also returns
+ * dJ/dcoeffs, dJ/dtau and dJ/dv_i from a hand-written discrete adjoint: the
+ * state is checkpointed every checkpoint_every steps, and the reverse sweep
+ * recomputes each segment from its checkpoint (memory ~ (T/K + K) states). */
+typedef struct {
+    int64_t n_steps;            /* T >= 1 */
+    int64_t checkpoint_every;   /* K >= 1; ignored without gradient */
+    int32_t precision;          /* LBM_STORE_F64 or LBM_STORE_F32: type of the state and adjoint */
+    int32_t n_target;
+    const int64_t* target;      /* [n_target] distinct entries of the near-wall list */
+    int32_t n_coeffs;
+    const double* basis;        /* [n_coeffs][n_inlet], caller's inlet order */
+    const double* coeffs;       /* [n_coeffs] */
+} lbm_adjoint_desc;
+
+typedef struct {
+    double objective;           /* J */
+    double dJ_dtau;             /* with gradient */
+    double* grad_coeffs;        /* caller-owned [n_coeffs], or NULL */
+    double* grad_inlet;         /* caller-owned [n_inlet] dJ/dv_i, or NULL */
+    double* final_populations;  /* caller-owned [n_nodes][q], f after the T steps, or NULL */
+    double forward_ms;          /* device time of the forward sweep */
+    double reverse_ms;          /* device time of recomputation and reverse sweep */
+    int64_t steps_recomputed;
+    int64_t device_bytes;       /* device memory the run allocated (freed on return) */
+} lbm_adjoint_result;
+
+int lbm_adjoint_run(lbm_engine* e, const lbm_adjoint_desc* desc, int32_t gradient, lbm_adjoint_result* result);
+
 /* Message of the last failed call on e (or of the last failed lbm_create when
  * e is NULL). Never NULL. */
 const char* lbm_last_error(const lbm_engine* e);

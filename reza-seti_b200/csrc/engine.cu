@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint.h"
 #include "errors.h"
 #include "lbm_b200.h"
 #include "launch.h"
@@ -973,6 +974,96 @@ int lbm_get_flags(lbm_engine* e, uint32_t* flags) {
     if (ce != cudaSuccess) return e->cuda_fail(ce, "download");
     if (int rc = sync(e)) return rc;
     *flags = v;
+    return 0;
+}
+
+int lbm_adjoint_run(lbm_engine* e, const lbm_adjoint_desc* d, int32_t gradient, lbm_adjoint_result* r) {
+    if (!e || !d || !r) return LBM_ERR_ARGUMENT;
+    if (e->bc != LBM_BC_PHYSICS) return e->fail(LBM_ERR_STATE, "the adjoint needs physics boundaries");
+    if (d->precision != LBM_STORE_F64 && d->precision != LBM_STORE_F32)
+        return e->fail(LBM_ERR_ARGUMENT, "adjoint precision must be LBM_STORE_F64 or LBM_STORE_F32");
+    if (d->n_steps < 1) return e->fail(LBM_ERR_ARGUMENT, "adjoint needs at least one step");
+    if (gradient && d->checkpoint_every < 1) return e->fail(LBM_ERR_ARGUMENT, "checkpoint interval below 1");
+    if (d->n_target < 0 || (d->n_target > 0 && !d->target)) return e->fail(LBM_ERR_ARGUMENT, "bad target list");
+    const int n_in = e->nin();
+    if (d->n_coeffs < 0 || (d->n_coeffs > 0 && (!d->coeffs || (n_in > 0 && !d->basis))))
+        return e->fail(LBM_ERR_ARGUMENT, "bad inlet coefficients or basis");
+    if (e->pop_step != e->step) return e->fail(LBM_ERR_STATE, "populations of the last step were not observed");
+    cudaSetDevice(e->device);
+    AdjointSetup s;
+    s.Q = e->Q;
+    s.fp64 = d->precision == LBM_STORE_F64;
+    s.gradient = gradient != 0;
+    s.n = e->t.n;
+    s.ld = e->t.ld;
+    s.meta = e->meta;
+    s.seg_base = e->seg_base;
+    s.seg_delta = e->seg_delta;
+    s.aux = e->aux;
+    for (int c = 0; c < 3; ++c) s.in_normal[c] = e->inlet_normal[c];
+    s.n_in = n_in;
+    s.out_nrm = e->out_nrm;
+    s.out_rho = e->out_rho;
+    s.n_nw = e->nw();
+    s.nw_node = e->nw_node;
+    s.nw_normal = e->nw_normal;
+    s.wss_c = e->wss_c;
+    s.tau = e->tau;
+    s.f0 = e->obs_pop;
+    s.n_steps = d->n_steps;
+    s.checkpoint_every = d->checkpoint_every;
+    s.stream = e->stream;
+    // waveform factor of each step, as the engine's own steps from here would use it
+    const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
+    s.factors.resize((size_t)d->n_steps);
+    for (int64_t i = 0; i < d->n_steps; ++i)
+        s.factors[(size_t)i] = inlet_factor(e, e->step + i, pulsatile ? e->runtime + (double)i * e->dt : e->runtime);
+    s.speed.assign(n_in, 0.0);
+    for (int j = 0; j < d->n_coeffs; ++j)
+        for (int i = 0; i < n_in; ++i) s.speed[i] += d->coeffs[j] * d->basis[(size_t)j * n_in + i];
+    s.targets.resize(d->n_target);
+    for (int k = 0; k < d->n_target; ++k) {
+        if (d->target[k] < 0 || d->target[k] >= e->nw()) return e->fail(LBM_ERR_ARGUMENT, "target outside the near-wall list");
+        s.targets[k] = (int)d->target[k];
+    }
+    double* fin = nullptr;
+    if (r->final_populations) {
+        cudaError_t ce = cudaMalloc(&fin, sizeof(double) * (size_t)e->Q * e->t.ld);
+        if (ce != cudaSuccess) return e->cuda_fail(ce, "adjoint output buffer");
+        s.final_pop = fin;
+    }
+    AdjointOut o;
+    const int rc = adjoint_run(s, o);
+    int status = 0;
+    if (rc == -1) status = e->fail(LBM_ERR_ARGUMENT, o.err);
+    else if (rc != 0) status = e->fail(LBM_ERR_CUDA, o.err);
+    if (!status && fin) {
+        status = ensure_staging(e);
+        if (!status) {
+            cudaError_t ce = launch_pop_to_caller(fin, e->perm, e->t.n, e->Q, e->t.ld, e->staging, e->stream);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(r->final_populations, e->staging, sizeof(double) * e->t.n * e->Q,
+                                     cudaMemcpyDeviceToHost, e->stream);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+            if (ce != cudaSuccess) status = e->cuda_fail(ce, "adjoint populations");
+        }
+    }
+    if (fin) cudaFree(fin);
+    if (status) return status;
+    r->objective = o.J;
+    r->dJ_dtau = s.gradient ? -o.dJ_domega / (e->tau * e->tau) : 0.0;
+    if (r->grad_coeffs)
+        for (int j = 0; j < d->n_coeffs; ++j) {
+            double g = 0.0;
+            for (int i = 0; i < n_in; ++i) g += d->basis[(size_t)j * n_in + i] * o.dJ_dspeed[i];
+            r->grad_coeffs[j] = g;
+        }
+    if (r->grad_inlet)
+        for (int i = 0; i < n_in; ++i) r->grad_inlet[i] = o.dJ_dspeed[i];
+    r->forward_ms = o.forward_ms;
+    r->reverse_ms = o.reverse_ms;
+    r->steps_recomputed = o.steps_recomputed;
+    r->device_bytes = (int64_t)o.bytes;
     return 0;
 }
 

@@ -44,6 +44,23 @@ class LbmDesc(ctypes.Structure):
     ]
 
 
+class LbmAdjointDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_steps", ctypes.c_int64), ("checkpoint_every", ctypes.c_int64), ("precision", ctypes.c_int32),
+        ("n_target", ctypes.c_int32), ("target", _i64p), ("n_coeffs", ctypes.c_int32),
+        ("basis", _f64p), ("coeffs", _f64p),
+    ]
+
+
+class LbmAdjointResult(ctypes.Structure):
+    _fields_ = [
+        ("objective", ctypes.c_double), ("dJ_dtau", ctypes.c_double), ("grad_coeffs", _f64p),
+        ("grad_inlet", _f64p), ("final_populations", _f64p), ("forward_ms", ctypes.c_double),
+        ("reverse_ms", ctypes.c_double), ("steps_recomputed", ctypes.c_int64),
+        ("device_bytes", ctypes.c_int64),
+    ]
+
+
 class LbmError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__("lbm error %d: %s" % (code, msg))
@@ -77,6 +94,8 @@ SIGNATURES = {
     "lbm_get_flags": (ctypes.c_int, [_E, ctypes.POINTER(ctypes.c_uint32)]),
     "lbm_step_timed": (ctypes.c_int, [_E, ctypes.c_int64, _f64p, _f64p]),
     "lbm_get_info": (ctypes.c_int, [_E, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),
+    "lbm_adjoint_run": (ctypes.c_int, [_E, ctypes.POINTER(LbmAdjointDesc), ctypes.c_int32,
+                                       ctypes.POINTER(LbmAdjointResult)]),
     "lbm_last_error": (ctypes.c_char_p, [_E]),
 }
 

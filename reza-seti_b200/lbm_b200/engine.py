@@ -179,6 +179,40 @@ class Engine:
         self._check(capi.lib().lbm_get_flags(self._h, ctypes.byref(v)))
         return v.value
 
+    def adjoint(self, n_steps, targets, basis, coeffs, *, gradient=True, checkpoint_every=100,
+                precision="f32", final_populations=False):
+        """Time-averaged WSS^2 objective over the near-wall entries `targets`
+        and, with `gradient`, its adjoint gradient (lbm_adjoint_run). The
+        inlet speed along -inlet_normal is coeffs @ basis ([n_coeffs, n_inlet]).
+        Returns a dict: J, dJ_dtau, grad_coeffs, grad_inlet, forward_ms,
+        reverse_ms, steps_recomputed, device_bytes (and populations)."""
+        targets = np.ascontiguousarray(targets, dtype=np.int64).reshape(-1)
+        basis = np.ascontiguousarray(basis, dtype=np.float64).reshape(-1, self.n_inlet)
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.float64).reshape(-1)
+        if len(coeffs) != basis.shape[0]:
+            raise ValueError("one coefficient per basis row")
+        d = capi.LbmAdjointDesc()
+        d.n_steps, d.checkpoint_every = int(n_steps), int(checkpoint_every)
+        d.precision = capi.STORAGE[precision]
+        d.n_target, d.target = len(targets), _p(targets, capi._i64p)
+        d.n_coeffs, d.basis, d.coeffs = len(coeffs), _p(basis, capi._f64p), _p(coeffs, capi._f64p)
+        gc = np.zeros(max(1, len(coeffs)))
+        gi = np.zeros(max(1, self.n_inlet))
+        r = capi.LbmAdjointResult()
+        r.grad_coeffs, r.grad_inlet = _p(gc, capi._f64p), _p(gi, capi._f64p)
+        fp = None
+        if final_populations:
+            fp = np.empty((self.n, self.q))
+            r.final_populations = _p(fp, capi._f64p)
+        self._check(capi.lib().lbm_adjoint_run(self._h, ctypes.byref(d), int(bool(gradient)), ctypes.byref(r)))
+        out = {"J": r.objective, "dJ_dtau": r.dJ_dtau, "grad_coeffs": gc[: len(coeffs)].copy(),
+               "grad_inlet": gi[: self.n_inlet].copy(), "forward_ms": r.forward_ms,
+               "reverse_ms": r.reverse_ms, "steps_recomputed": r.steps_recomputed,
+               "device_bytes": r.device_bytes}
+        if fp is not None:
+            out["populations"] = fp
+        return out
+
     def info(self):
         vals = [ctypes.c_int64() for _ in range(6)]
         self._check(capi.lib().lbm_get_info(self._h, *[ctypes.byref(v) for v in vals]))

@@ -223,6 +223,38 @@ def straight_pipe(radius=16.0, length=128, box=None, centre=None, stenosis=0.0, 
     return topo
 
 
+def zernike_inlet_basis(topo, n=8, radius=None, centre=None):
+    """Zernike-like inlet speed modes on the pipe's inlet disc, [n, n_inlet]:
+    the low-order Zernike polynomials (1, rho cos t, rho sin t, 2 rho^2 - 1,
+    rho^2 cos 2t, rho^2 sin 2t, (3 rho^3 - 2 rho) cos t, (3 rho^3 - 2 rho) sin t,
+    ...) times (1 - rho^2), so every mode vanishes on the wall; zero outside
+    the radius. Mode 0 is the Poiseuille profile with unit peak."""
+    R = float(topo["radius"][0]) if radius is None else radius
+    cx, cy = topo["axis_centre"] if centre is None else centre
+    xy = topo["coords"][topo["inlet"]][:, :2].astype(np.float64)
+    dx, dy = xy[:, 0] - cx, xy[:, 1] - cy
+    rho = np.hypot(dx, dy) / R
+    th = np.arctan2(dy, dx)
+    modes = [np.ones_like(rho), rho * np.cos(th), rho * np.sin(th), 2 * rho ** 2 - 1,
+             rho ** 2 * np.cos(2 * th), rho ** 2 * np.sin(2 * th),
+             (3 * rho ** 3 - 2 * rho) * np.cos(th), (3 * rho ** 3 - 2 * rho) * np.sin(th),
+             6 * rho ** 4 - 6 * rho ** 2 + 1, rho ** 3 * np.cos(3 * th), rho ** 3 * np.sin(3 * th)]
+    if n > len(modes):
+        raise ValueError("at most %d modes" % len(modes))
+    env = np.maximum(0.0, 1.0 - rho ** 2)
+    return np.stack([m * env for m in modes[:n]])
+
+
+def stenotic_throat_targets(topo, half_length, z_centre=None):
+    """Near-wall list entries within half_length of the throat plane (z =
+    length / 2 by default, where straight_pipe centres its stenosis), [k]
+    int64."""
+    nw = np.asarray(topo["nearwall"], dtype=np.int64)
+    z = topo["coords"][nw][:, 2].astype(np.float64)
+    zc = (float(topo["coords"][:, 2].max()) + 1.0) / 2 if z_centre is None else z_centre
+    return np.nonzero(np.abs(z - zc) <= half_length)[0].astype(np.int64)
+
+
 def parabolic_inlet(topo, u_max, radius=None, centre=None):
     """Poiseuille inlet profile along +z for the inlet nodes of a pipe:
     u_z = u_max (1 - r^2 / R^2), zero outside R ([n_inlet, 3])."""

@@ -1,0 +1,168 @@
+"""Adjoint of the physics-mode step (lbm_adjoint_run).
+
+The objective J = (1/T) sum_t sum_{throat} |tau|^2 and its gradient with
+respect to Zernike-like inlet coefficients and tau, on a stenosed pipe:
+  * the adjoint's forward sweep equals the engine's own physics-mode steps
+    (populations and the per-step wall shear stress, FP64);
+  * the FP64 adjoint gradient equals central finite differences (h = 1e-4) of
+    the FP64 objective, for D3Q19 and D3Q27;
+  * the FP32 adjoint gradient is within 1e-3 of the FP64 one;
+  * the gradient does not depend on the checkpoint interval.
+"""
+import numpy as np
+import pytest
+
+from lbm_b200 import Engine, capi
+from lbm_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-4          # finite-difference step (coefficients and tau)
+PERIOD, AMP, PHASE = 50.0, [0.3, 0.1], [0.0, 1.0]
+
+
+def stenosed_pipe():
+    return G.straight_pipe(radius=6.0, length=40, stenosis=0.4, stenosis_sigma=4.0)
+
+
+def coefficients(n=8, seed=7):
+    rng = np.random.default_rng(seed)
+    a = 0.002 * rng.standard_normal(n)
+    a[0] = 0.03
+    return a
+
+
+def physics_engine(topo, tau, q=19, harmonic=True):
+    e = Engine(topo, tau=tau, lattice=q, storage="f64", bc="physics")
+    if harmonic:
+        e.set_waveform(PERIOD, AMP, PHASE)
+        e.set_flow(False, 0.0, harmonic=True)
+    return e
+
+
+def inflow_direction(topo):
+    return -np.asarray(topo["inlet_normal"], dtype=np.float64).reshape(3)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def fd_gradient(topo, q, tau, T, targets, basis, a):
+    e = physics_engine(topo, tau, q)
+    g = np.zeros(len(a))
+    for j in range(len(a)):
+        ap, am = a.copy(), a.copy()
+        ap[j] += H
+        am[j] -= H
+        jp = e.adjoint(T, targets, basis, ap, gradient=False, precision="f64")["J"]
+        jm = e.adjoint(T, targets, basis, am, gradient=False, precision="f64")["J"]
+        g[j] = (jp - jm) / (2 * H)
+    def j_tau(t):
+        return physics_engine(topo, t, q).adjoint(T, targets, basis, a, gradient=False, precision="f64")["J"]
+
+    gt = [(j_tau(tau + h) - j_tau(tau - h)) / (2 * h) for h in (H, H / 2)]
+    return g, gt[0], (4 * gt[1] - gt[0]) / 3
+
+
+def test_forward_sweep_equals_engine_steps():
+    """From a developed state (7 engine steps in), T steps of the adjoint's
+    forward sweep give the engine's populations, and J equals the mean over
+    the steps of the engine's |WSS|^2 summed over the throat nodes."""
+    topo = stenosed_pipe()
+    basis = G.zernike_inlet_basis(topo, 8)
+    a = coefficients()
+    targets = G.stenotic_throat_targets(topo, 4.0)
+    assert len(targets) > 20
+    e = physics_engine(topo, 0.6)
+    e.set_inlet_profile((a @ basis)[:, None] * inflow_direction(topo)[None, :])
+    e.step(7)
+    T = 40
+    r = e.adjoint(T, targets, basis, a, gradient=False, precision="f64", final_populations=True)
+    J = 0.0
+    for _ in range(T):
+        e.step(1)
+        J += float(np.sum(e.wss()[0][targets] ** 2))
+    J /= T
+    f = e.populations()
+    assert np.max(np.abs(r["populations"] - f)) < 1e-13 * np.max(np.abs(f))
+    assert abs(r["J"] - J) < 1e-9 * J
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_fp64_adjoint_matches_central_differences(q):
+    topo = stenosed_pipe()
+    basis = G.zernike_inlet_basis(topo, 8)
+    a = coefficients()
+    targets = G.stenotic_throat_targets(topo, 4.0)
+    tau, T = 0.6, 120 if q == 19 else 80
+    e = physics_engine(topo, tau, q)
+    r = e.adjoint(T, targets, basis, a, gradient=True, checkpoint_every=25, precision="f64")
+    assert r["steps_recomputed"] == ((T - 1) // 25) * 25  # every segment but the last
+    g_fd, gt_fd, gt_rich = fd_gradient(topo, q, tau, T, targets, basis, a)
+    # every component against the largest, and the whole vector
+    assert np.max(np.abs(r["grad_coeffs"] - g_fd)) < 1e-6 * np.max(np.abs(g_fd))
+    assert rel(r["grad_coeffs"], g_fd) < 1e-6
+    # J is far from quadratic in tau: the h = 1e-4 difference carries a
+    # truncation error h^2 J''' / 6 of about 1e-6 relative, which the
+    # Richardson combination of h and h/2 removes
+    assert abs(r["dJ_dtau"] - gt_fd) < 1e-5 * abs(gt_fd)
+    assert abs(r["dJ_dtau"] - gt_rich) < 1e-8 * abs(gt_rich)
+    np.testing.assert_allclose(r["grad_coeffs"], basis @ r["grad_inlet"], rtol=1e-12,
+                               atol=1e-14 * np.max(np.abs(r["grad_coeffs"])))
+
+
+def test_fp32_adjoint_tracks_fp64():
+    topo = stenosed_pipe()
+    basis = G.zernike_inlet_basis(topo, 8)
+    a = coefficients()
+    targets = G.stenotic_throat_targets(topo, 4.0)
+    e = physics_engine(topo, 0.6)
+    r64 = e.adjoint(200, targets, basis, a, checkpoint_every=30, precision="f64")
+    r32 = e.adjoint(200, targets, basis, a, checkpoint_every=30, precision="f32")
+    assert abs(r32["J"] - r64["J"]) < 1e-4 * r64["J"]
+    assert rel(r32["grad_coeffs"], r64["grad_coeffs"]) < 1e-3
+    assert abs(r32["dJ_dtau"] - r64["dJ_dtau"]) < 1e-3 * abs(r64["dJ_dtau"])
+
+
+def test_gradient_independent_of_checkpoint_interval():
+    topo = stenosed_pipe()
+    basis = G.zernike_inlet_basis(topo, 8)
+    a = coefficients()
+    targets = G.stenotic_throat_targets(topo, 4.0)
+    e = physics_engine(topo, 0.6)
+    T = 60
+    runs = [e.adjoint(T, targets, basis, a, checkpoint_every=k, precision="f64") for k in (1, 7, 60, 1000)]
+    for r in runs[1:]:
+        assert r["J"] == pytest.approx(runs[0]["J"], rel=1e-14)
+        np.testing.assert_allclose(r["grad_inlet"], runs[0]["grad_inlet"], rtol=1e-13, atol=0)
+        assert r["dJ_dtau"] == pytest.approx(runs[0]["dJ_dtau"], rel=1e-13)
+    assert runs[0]["steps_recomputed"] == T - 1 and runs[2]["steps_recomputed"] == 0
+
+
+def test_argument_and_state_errors():
+    topo = stenosed_pipe()
+    basis = G.zernike_inlet_basis(topo, 2)
+    a = coefficients(2)
+    e = physics_engine(topo, 0.6)
+    with pytest.raises(capi.LbmError) as ex:
+        e.adjoint(10, [0, 0], basis, a)
+    assert ex.value.code == capi.LBM_ERR_ARGUMENT
+    with pytest.raises(capi.LbmError) as ex:
+        e.adjoint(10, [e.n_nearwall], basis, a)
+    assert ex.value.code == capi.LBM_ERR_ARGUMENT
+    with pytest.raises(capi.LbmError) as ex:
+        e.adjoint(10, [0], basis, a, precision="f16")
+    assert ex.value.code == capi.LBM_ERR_ARGUMENT
+    with pytest.raises(capi.LbmError) as ex:
+        e.adjoint(0, [0], basis, a)
+    assert ex.value.code == capi.LBM_ERR_ARGUMENT
+    ref = Engine(topo, tau=0.6, storage="f64", bc="reference")
+    with pytest.raises(capi.LbmError) as ex:
+        ref.adjoint(10, [0], basis, a)
+    assert ex.value.code == capi.LBM_ERR_STATE
+    e.set_observation(0)
+    e.step(3)
+    with pytest.raises(capi.LbmError) as ex:
+        e.adjoint(10, [0], basis, a)
+    assert ex.value.code == capi.LBM_ERR_STATE

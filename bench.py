@@ -257,6 +257,13 @@ def run_gpu(args):
     if rank == 0 and not args.no_variants:
         variants = run_variants(args, topo, n, torch, device, vel, radius)
 
+    precision = None
+    if rank == 0 and not args.no_precision:
+        precision = run_precision(torch, device)
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        adjoint = run_adjoint(torch, device)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference(args, sample_only=True)
@@ -278,7 +285,7 @@ def run_gpu(args):
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": 2 * args.steps, "clocks": clocks, "device_flags": flags,
-            "variants": variants,
+            "variants": variants, "precision": precision, "adjoint": adjoint,
         }
         print(json.dumps(line))
     if dist:
@@ -334,6 +341,159 @@ def run_variants(args, topo, n, torch, device, vel, radius):
                               "step_kernel_GBs": round(2 * 19 * 4 * n / (ms_step / steps / 1e3) / 1e9, 1),
                               "device_flags": eng.flags()}
     eng.close()
+    return out
+
+
+# --------------------------------------------------------------- precision ---
+PRECISION_PERIOD = 4000
+PRECISION_PERIODS = 2
+
+
+def harmonic_waveform(seed=3, n=4):
+    """Seeded Womersley-type waveform: harmonic k (1-based) with amplitude
+    uniform in [0, 0.5] / k of the mean and a uniform phase."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.0, 0.5, n) / np.arange(1, n + 1)
+    phase = rng.uniform(0.0, 2 * np.pi, n)
+    return amp, phase
+
+
+def run_precision(torch, device, topo=None):
+    """TAWSS / OSI (FP64 accumulators) and final-state errors of FP32, FP16 and
+    BF16 storage against FP64 storage, on the radius-20 tortuous vessel over
+    two periods of a 4-harmonic waveform (tau 0.52, Re 300 at the mean flow).
+    Errors are relative L2 norms over all near-wall nodes (TAWSS, WSS),
+    over all nodes (velocity, populations f - w), and max |OSI| differences."""
+    from lbm_b200 import Engine
+    from lbm_b200 import geometry as G
+    r = 20.0
+    if topo is None:
+        topo = G.tortuous_vessel(radius=r, box=BOX)
+    n = len(topo["kind"])
+    vel = inlet_velocity(r)
+    amp, phase = harmonic_waveform()
+    steps = PRECISION_PERIOD * PRECISION_PERIODS
+    w = np.array([2 / 36] * 6 + [1 / 36] * 12 + [12 / 36])
+
+    def l2(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    out = {"workload": "tortuous stenosed vessel radius 20 lu, 512x512x1024 box (%d fluid nodes)" % n,
+           "steps": steps, "waveform": {"period_steps": PRECISION_PERIOD, "amplitude": np.round(amp, 4).tolist(),
+                                        "phase": np.round(phase, 4).tolist(), "seed": 3},
+           "tau": TAU, "mean_inlet_velocity": round(vel, 6)}
+    ref = None
+    for storage in ("f64", "f32", "f16", "bf16"):
+        eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device, bc="physics")
+        eng.set_inlet_profile(inlet_profile(topo, r, vel))
+        eng.set_waveform(float(PRECISION_PERIOD), amp, phase)
+        eng.set_flow(False, vel, harmonic=True)
+        t0 = time.perf_counter()
+        eng.step(steps)
+        osi, tawss = eng.osi_tawss()
+        wss = eng.wss()[0]
+        d = eng.populations() - w
+        u = eng.macros()[1]
+        flags = eng.flags()
+        secs = time.perf_counter() - t0
+        eng.close()
+        row = {"seconds": round(secs, 2), "device_flags": flags}
+        if ref is None:
+            ref = (osi, tawss, wss, d, u)
+            row["tawss_mean"] = float(np.mean(tawss))
+            row["osi_max"] = float(np.max(osi))
+        else:
+            row.update({"tawss_rel_l2": l2(tawss, ref[1]),
+                        "tawss_rel_max": float(np.max(np.abs(tawss - ref[1])) / np.max(np.abs(ref[1]))),
+                        "osi_abs_max": float(np.max(np.abs(osi - ref[0]))),
+                        "wss_rel_l2": l2(wss, ref[2]), "velocity_rel_l2": l2(u, ref[4]),
+                        "populations_rel_l2": l2(d, ref[3])})
+        out[storage] = row
+    return out
+
+
+# ----------------------------------------------------------------- adjoint ---
+ADJ_STEPS, ADJ_K, ADJ_TAU = 3000, 100, 0.6
+
+
+def adjoint_workload():
+    """Stenosed pipe: radius 24 lu in a 64 x 64 x 384 box, Gaussian stenosis
+    narrowing the radius by 60 % at mid-length (sigma 12 lu); objective over
+    the near-wall nodes within 12 lu of the throat; 8 Zernike-like inlet modes
+    with seeded coefficients (mode 0 peak 0.012 lu)."""
+    from lbm_b200 import geometry as G
+    topo = G.straight_pipe(radius=24.0, length=384, box=(64, 64, 384), stenosis=0.6, stenosis_sigma=12.0)
+    basis = G.zernike_inlet_basis(topo, 8)
+    rng = np.random.default_rng(11)
+    a = 0.0012 * rng.standard_normal(8)
+    a[0] = 0.012
+    targets = G.stenotic_throat_targets(topo, 12.0)
+    return topo, basis, a, targets
+
+
+def run_adjoint(torch, device, fd=True):
+    """Adjoint gradient of the throat's time-averaged WSS^2 w.r.t. 8 inlet
+    coefficients and tau (3000 steps, checkpoint every 100): FP32 cost per
+    step against the engine's FP32 forward step on the same pipe, and
+    accuracy against an FP64 adjoint and central differences (h = 1e-4) of
+    the FP64 objective."""
+    from lbm_b200 import Engine
+    topo, basis, a, targets = adjoint_workload()
+    n = len(topo["kind"])
+
+    def engine(tau, storage="f64"):
+        e = Engine(topo, tau=tau, dt=1e-5, spacing=1.0, storage=storage, device=device, bc="physics")
+        return e
+
+    # the engine's own FP32 forward step on this geometry (inlet = the same modes)
+    fw = engine(ADJ_TAU, "f32")
+    fw.set_inlet_profile((a @ basis)[:, None] * -np.asarray(topo["inlet_normal"], dtype=np.float64)[None, :])
+    fw.set_observation(False)
+    fw.step(20)
+    ms_step, ms_bnd = fw.step_timed(ADJ_STEPS)
+    fw.close()
+    fwd_ms = (ms_step + ms_bnd) / ADJ_STEPS
+
+    e = engine(ADJ_TAU)
+    e.adjoint(50, targets, basis, a, checkpoint_every=10, precision="f32")   # warm-up
+    r32 = e.adjoint(ADJ_STEPS, targets, basis, a, checkpoint_every=ADJ_K, precision="f32")
+    r64 = e.adjoint(ADJ_STEPS, targets, basis, a, checkpoint_every=ADJ_K, precision="f64")
+    g32 = np.append(r32["grad_coeffs"], r32["dJ_dtau"])
+    g64 = np.append(r64["grad_coeffs"], r64["dJ_dtau"])
+    total32 = r32["forward_ms"] + r32["reverse_ms"]
+    out = {"workload": "stenosed pipe R=24 lu, 64x64x384 box, 60%% radius stenosis; %d fluid nodes, "
+                       "%d throat near-wall nodes" % (n, len(targets)),
+           "steps": ADJ_STEPS, "checkpoint_every": ADJ_K, "tau": ADJ_TAU, "parameters": "8 inlet modes + tau",
+           "J_f32": r32["J"], "J_f64": r64["J"],
+           "engine_forward_step_ms_f32": round(fwd_ms, 5),
+           "adjoint_ms_f32": {"forward_sweep": round(r32["forward_ms"], 2),
+                              "recompute_and_reverse": round(r32["reverse_ms"], 2)},
+           "steps_recomputed": r32["steps_recomputed"],
+           "cost_per_step_vs_forward_step": round(total32 / ADJ_STEPS / fwd_ms, 3),
+           "device_bytes_f32": r32["device_bytes"],
+           "grad_f32_vs_f64_rel": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+           "grad_f64": g64.tolist()}
+    if fd:
+        h = 1e-4
+        g_fd = np.zeros(9)
+        for j in range(8):
+            ap, am = a.copy(), a.copy()
+            ap[j] += h
+            am[j] -= h
+            g_fd[j] = (e.adjoint(ADJ_STEPS, targets, basis, ap, gradient=False, precision="f64")["J"] -
+                       e.adjoint(ADJ_STEPS, targets, basis, am, gradient=False, precision="f64")["J"]) / (2 * h)
+        jt = []
+        for t in (ADJ_TAU + h, ADJ_TAU - h):
+            et = engine(t)
+            jt.append(et.adjoint(ADJ_STEPS, targets, basis, a, gradient=False, precision="f64")["J"])
+            et.close()
+        g_fd[8] = (jt[0] - jt[1]) / (2 * h)
+        out["fd_h"] = h
+        out["grad_fd"] = g_fd.tolist()
+        out["f64_vs_fd_rel"] = float(np.linalg.norm(g64 - g_fd) / np.linalg.norm(g_fd))
+        out["f32_vs_fd_rel"] = float(np.linalg.norm(g32 - g_fd) / np.linalg.norm(g_fd))
+        out["f64_vs_fd_rel_per_parameter"] = (np.abs(g64 - g_fd) / np.abs(g_fd)).round(8).tolist()
+    e.close()
     return out
 
 
@@ -450,11 +610,20 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--section", default="all", choices=["all", "precision", "adjoint"],
+                    help="run only the precision study or only the adjoint measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.section != "all":
+        import torch
+        torch.cuda.set_device(0)
+        res = run_precision(torch, 0) if args.section == "precision" else run_adjoint(torch, 0)
+        print(json.dumps({"section": args.section, **res}))
     else:
         run_gpu(args)
 

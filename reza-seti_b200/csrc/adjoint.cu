@@ -268,7 +268,11 @@ __global__ void adj_objective_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, i
     if (threadIdx.x == 0 && s != 0.0) atomicAdd(a.J, s);
 }
 
-// lambda^t from lambda^{t+1} at every node (the transpose of the push).
+// lambda^t from lambda^{t+1} at every node (the transpose of the push). One
+// pass gathers mu (bounce-back links take the node's own lambda^{t+1}, negated
+// on outlet links) while it accumulates the moments of f^t and sum mu d; the
+// outlet velocity terms and the collision Jacobian follow from mu alone, so
+// the node's populations are never held as an array.
 template <class R, int Q>
 __global__ void __launch_bounds__(AT) adj_pull_kernel(AGeom<R, Q> g, const R* __restrict__ D,
                                                        const R* __restrict__ Ln, R* __restrict__ Lc, double s_t,
@@ -280,59 +284,73 @@ __global__ void __launch_bounds__(AT) adj_pull_kernel(AGeom<R, Q> g, const R* __
     if (n < g.n) {
         const auto m = g.meta[n];
         const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
-        R d[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) d[q] = D[(long long)q * g.ld + n];
-        R drho, u[3];
-        dmoments<R, Q>(d, drho, u);
         const int* sd = nbr_row<Q>(g.seg_base, g.seg_delta, n, m);
-        double nrm[3] = {0, 0, 0};
+        R nrm[3] = {R(0), R(0), R(0)};
         if (kind == KIND_INLET) {
-            for (int c = 0; c < 3; ++c) nrm[c] = g.in_normal[c];
+            for (int c = 0; c < 3; ++c) nrm[c] = (R)g.in_normal[c];
         } else if (kind == KIND_OUTLET) {
-            for (int c = 0; c < 3; ++c) nrm[c] = g.out_nrm[3 * (long long)g.aux[n] + c];
+            for (int c = 0; c < 3; ++c) nrm[c] = (R)g.out_nrm[3 * (long long)g.aux[n] + c];
         }
         R mu[Q];
-        R G[3] = {R(0), R(0), R(0)};
-        double gin = 0.0;
+        R drho = R(0), j0 = R(0), j1 = R(0), j2 = R(0), mud = R(0), gin = R(0);
+        unsigned out_links = 0;  // bit q: q is an outlet link (mu_q = -lambda)
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
+            const R dq = D[(long long)q * g.ld + n];
+            drho += dq;
+            if (L::cx(q)) j0 += L::cx(q) > 0 ? dq : -dq;
+            if (L::cy(q)) j1 += L::cy(q) > 0 ? dq : -dq;
+            if (L::cz(q)) j2 += L::cz(q) > 0 ? dq : -dq;
+            R v;
             if (q == L::REST) {
-                mu[q] = Ln[(long long)q * g.ld + n];
+                v = Ln[(long long)q * g.ld + n];
             } else if ((m >> q) & 1) {
-                mu[q] = Ln[(long long)q * g.ld + (n + sd[q])];
+                v = Ln[(long long)q * g.ld + (n + sd[q])];
             } else {
-                const R l = Ln[(long long)L::opp(q) * g.ld + n];
-                mu[q] = l;
-                const double cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
-                if (cn > 0.0) {
+                v = Ln[(long long)L::opp(q) * g.ld + n];
+                const R cn = R(L::cx(q)) * nrm[0] + R(L::cy(q)) * nrm[1] + R(L::cz(q)) * nrm[2];
+                if (cn > R(0)) {
                     if (kind == KIND_INLET) {
-                        gin += (double)l * 6.0 * L::w(q) * cn * s_t;
+                        gin += v * R(6.0 * L::w(q)) * cn;
                     } else {
-                        mu[q] = -l;
-                        const R c0 = R(L::cx(q)), c1 = R(L::cy(q)), c2 = R(L::cz(q));
-                        const R cu = c0 * u[0] + c1 * u[1] + c2 * u[2];
-                        const R k = l * R(2.0 * L::w(q) * g.out_rho);
-                        G[0] += k * (R(9) * cu * c0 - R(3) * u[0]);
-                        G[1] += k * (R(9) * cu * c1 - R(3) * u[1]);
-                        G[2] += k * (R(9) * cu * c2 - R(3) * u[2]);
+                        v = -v;
+                        out_links |= 1u << q;
                     }
                 }
+            }
+            mu[q] = v;
+            mud += v * dq;
+        }
+        const R irho = R(1) / (R(1) + drho);
+        const R u[3] = {j0 * irho, j1 * irho, j2 * irho};
+        // outlet links: d/du of 2 w rho_out eq(u), times lambda = -mu
+        R G[3] = {R(0), R(0), R(0)};
+        if (out_links) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                if (!((out_links >> q) & 1)) continue;
+                const R c0 = R(L::cx(q)), c1 = R(L::cy(q)), c2 = R(L::cz(q));
+                const R cu = c0 * u[0] + c1 * u[1] + c2 * u[2];
+                const R k = -mu[q] * R(2.0 * L::w(q) * g.out_rho);
+                G[0] += k * (R(9) * cu * c0 - R(3) * u[0]);
+                G[1] += k * (R(9) * cu * c1 - R(3) * u[1]);
+                G[2] += k * (R(9) * cu * c2 - R(3) * u[2]);
             }
         }
         R A, B[3];
         feq_adjoint<R, Q>(mu, u, A, B);
         const R om = g.omega;
-        const R irho = R(1) / (R(1) + drho);
         const R gu = G[0] * u[0] + G[1] * u[1] + G[2] * u[2];
+        R mueq = R(0);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            wl += (double)mu[q] * (double)(deq<R, Q>(q, drho, u) - d[q]);
+            mueq += mu[q] * deq<R, Q>(q, drho, u);
             const R cb = R(L::cx(q)) * B[0] + R(L::cy(q)) * B[1] + R(L::cz(q)) * B[2];
             const R cg = R(L::cx(q)) * G[0] + R(L::cy(q)) * G[1] + R(L::cz(q)) * G[2];
             Lc[(long long)q * g.ld + n] = (R(1) - om) * mu[q] + om * (A + cb) + (cg - gu) * irho;
         }
-        if (kind == KIND_INLET) dspeed[g.aux[n]] += gin;
+        wl = (double)(mueq - mud);
+        if (kind == KIND_INLET) dspeed[g.aux[n]] += (double)gin * s_t;
     }
     const double s = block_sum(wl, red);
     if (threadIdx.x == 0 && s != 0.0) atomicAdd(domega, s);

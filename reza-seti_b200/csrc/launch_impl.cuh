@@ -3,6 +3,7 @@
 #pragma once
 
 #include "launch.h"
+#include "pair.cuh"
 
 namespace lbm {
 
@@ -19,8 +20,64 @@ static cudaError_t step_obs(const StepArgs<S, Q>& a, int obs, dim3 g, cudaStream
 }
 
 template <class S, int Q>
+static cudaError_t pair_phase0(const StepArgs<S, Q>& a, int obs, dim3 g, cudaStream_t st) {
+    switch (obs) {
+        case 0: pair_phase0_kernel<S, Q, 0><<<g, PAIR_THREADS, 0, st>>>(a); break;
+        case 1: pair_phase0_kernel<S, Q, 1><<<g, PAIR_THREADS, 0, st>>>(a); break;
+        case 2: pair_phase0_kernel<S, Q, 2><<<g, PAIR_THREADS, 0, st>>>(a); break;
+        default: pair_phase0_kernel<S, Q, 3><<<g, PAIR_THREADS, 0, st>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+// Persistent phase-1 pair kernel: one CTA per resident slot (SM count times
+// the occupancy at its shared-memory size), cached per host thread.
+template <class S, int Q, int OBS>
+static cudaError_t pair_phase1_launch(const StepArgs<S, Q>& a, cudaStream_t st) {
+    auto kern = pair_phase1_kernel<S, Q, OBS>;
+    const int n_tiles = (a.n + BLOCK_NODES - 1) / BLOCK_NODES;
+    const int smem = 2 * pair_buffer_bytes<Q>(a.seg_smem_bytes);
+    static thread_local int cached_dev = -1, cached_smem = -1, cached_grid = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev != cached_dev || smem != cached_smem) {
+        if (smem > 48 * 1024) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return e;
+        }
+        int sms = 0, per_sm = 0;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PAIR_THREADS, smem)) != cudaSuccess)
+            return e;
+        cached_grid = sms * (per_sm > 0 ? per_sm : 1);
+        cached_dev = dev;
+        cached_smem = smem;
+    }
+    const int grid = n_tiles < cached_grid ? n_tiles : cached_grid;
+    kern<<<grid, PAIR_THREADS, smem, st>>>(a, n_tiles);
+    return cudaGetLastError();
+}
+
+template <class S, int Q>
+static cudaError_t pair_phase1(const StepArgs<S, Q>& a, int obs, cudaStream_t st) {
+    switch (obs) {
+        case 0: return pair_phase1_launch<S, Q, 0>(a, st);
+        case 1: return pair_phase1_launch<S, Q, 1>(a, st);
+        case 2: return pair_phase1_launch<S, Q, 2>(a, st);
+        default: return pair_phase1_launch<S, Q, 3>(a, st);
+    }
+}
+
+template <class S, int Q>
 cudaError_t launch_step(const StepArgs<S, Q>& a, int phase, int bc, int obs, cudaStream_t st) {
     const dim3 g((a.n + BLOCK_NODES - 1) / BLOCK_NODES);
+    if constexpr (Store<S>::SHIFTED) {
+        // physics mode, shifted storage: two nodes per thread, 32-bit slot
+        // indices (lattices beyond 2^32 slots use step_kernel)
+        if (bc == BC_PHYSICS && (long long)Q * a.ld < (1LL << 32))
+            return phase ? pair_phase1<S, Q>(a, obs, st) : pair_phase0<S, Q>(a, obs, g, st);
+    }
     if (bc == BC_REFERENCE) {
         if constexpr (Q == 19) {
             return phase ? step_obs<S, Q, 1, BC_REFERENCE>(a, obs, g, st)

@@ -1,0 +1,330 @@
+// Physics-mode step kernels for shifted storage (FP32 / FP16 / BF16), two
+// nodes per thread.
+//
+// The nodes n and n + 1 of a thread are adjacent in memory (n even; ld is a
+// multiple of BLOCK_NODES), so:
+//  * phase 0 reads and writes both nodes' slots with one 2-wide access
+//    (float2, __half2, __nv_bfloat162): its slots (n, q) and (n, opp q) do not
+//    depend on the neighbours, and physics mode stores c_q into (n, opp q)
+//    whether or not the neighbour exists;
+//  * the collision of the two nodes runs in packed FP32 (fma.rn.f32x2 and
+//    friends), one instruction for both nodes. Opposite directions share
+//    c.u, so each direction pair costs one symmetric and one antisymmetric
+//    term.
+// Phase 1 gathers and scatters each node on its own (the neighbours' slots
+// are not pairwise aligned), with a select between the neighbour's slot and
+// the node's own opposite slot for missing neighbours, as in step_kernel.
+// Results equal step_kernel's up to FP32 rounding (the arithmetic is
+// rearranged).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace lbm {
+
+__device__ __forceinline__ float2 f2s(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return __ffma2_rn(b, f2s(-1.f), a); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// 2-wide and scalar access to the stored deviations, in FP32.
+template <class S>
+struct PairIO;
+template <>
+struct PairIO<float> {
+    __device__ static float2 get2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+    __device__ static void put2(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+    __device__ static float get(const float* p) { return *p; }
+    __device__ static void put(float* p, float v) { *p = v; }
+};
+template <>
+struct PairIO<__half> {
+    __device__ static float2 get2(const __half* p) { return __half22float2(*reinterpret_cast<const __half2*>(p)); }
+    __device__ static void put2(__half* p, float2 v) { *reinterpret_cast<__half2*>(p) = __float22half2_rn(v); }
+    __device__ static float get(const __half* p) { return __half2float(*p); }
+    __device__ static void put(__half* p, float v) { *p = __float2half_rn(v); }
+};
+template <>
+struct PairIO<__nv_bfloat16> {
+    __device__ static float2 get2(const __nv_bfloat16* p) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+    }
+    __device__ static void put2(__nv_bfloat16* p, float2 v) {
+        *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
+    }
+    __device__ static float get(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    __device__ static void put(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+constexpr int PAIR_THREADS = BLOCK_NODES / 2;
+
+// BGK collision of two nodes' deviations d (in place): c = (1 - omega) d +
+// omega deq, deq_q = w_q (drho + (1 + drho)(3 c.u + 4.5 (c.u)^2 - 1.5 u^2)).
+// Returns drho and u of the input.
+template <int Q>
+__device__ __forceinline__ void collide_pair(float2 d[Q], float omega, float2& drho, float2 u[3]) {
+    using L = Lat<Q>;
+    float2 ra = f2s(0.f), rb = f2s(0.f);
+    float2 j0 = f2s(0.f), j1 = f2s(0.f), j2 = f2s(0.f);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (q & 1) rb = f2add(rb, d[q]);
+        else ra = f2add(ra, d[q]);
+        if (L::cx(q)) j0 = L::cx(q) > 0 ? f2add(j0, d[q]) : f2sub(j0, d[q]);
+        if (L::cy(q)) j1 = L::cy(q) > 0 ? f2add(j1, d[q]) : f2sub(j1, d[q]);
+        if (L::cz(q)) j2 = L::cz(q) > 0 ? f2add(j2, d[q]) : f2sub(j2, d[q]);
+    }
+    drho = f2add(ra, rb);
+    const float2 rho = f2add(f2s(1.f), drho);
+    const float2 inv = make_float2(1.f / rho.x, 1.f / rho.y);
+    u[0] = f2mul(j0, inv);
+    u[1] = f2mul(j1, inv);
+    u[2] = f2mul(j2, inv);
+    const float2 usq = f2fma(u[0], u[0], f2fma(u[1], u[1], f2mul(u[2], u[2])));
+    // deq_q = w (base + rho 4.5 (c.u)^2 + 3 rho c.u), base = drho - 1.5 rho u^2
+    const float2 base = f2fma(rho, f2mul(f2s(-1.5f), usq), drho);
+    const float2 rho3 = f2mul(f2s(3.f), rho);
+    const float2 keep = f2s(1.f - omega);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int o = L::opp(q);
+        if (q == L::REST) {
+            d[q] = f2fma(keep, d[q], f2mul(f2s(omega * (float)L::w(q)), base));
+            continue;
+        }
+        if (o < q) continue;  // handled with its opposite
+        float2 cu = f2s(0.f);
+        bool first = true;
+        auto acc = [&](int c, float2 v) {
+            if (!c) return;
+            if (first) {
+                cu = c > 0 ? v : f2mul(f2s(-1.f), v);
+                first = false;
+            } else {
+                cu = c > 0 ? f2add(cu, v) : f2sub(cu, v);
+            }
+        };
+        acc(L::cx(q), u[0]);
+        acc(L::cy(q), u[1]);
+        acc(L::cz(q), u[2]);
+        const float2 sym = f2fma(rho, f2mul(f2mul(f2s(4.5f), cu), cu), base);
+        const float2 anti = f2mul(rho3, cu);
+        const float2 wo = f2s(omega * (float)L::w(q));
+        d[q] = f2fma(keep, d[q], f2mul(wo, f2add(sym, anti)));
+        d[o] = f2fma(keep, d[o], f2mul(wo, f2sub(sym, anti)));
+    }
+}
+
+// Everything between the gather and the scatter of a pair: observation,
+// near-wall hand-off, collision, non-finite flag, outlet velocities.
+template <class S, int Q, int OBS>
+__device__ __forceinline__ void pair_middle(const StepArgs<S, Q>& a, float2 s[Q], typename Meta<Q>::T m0,
+                                            typename Meta<Q>::T m1, int n0, bool live1) {
+    using L = Lat<Q>;
+    const int n1 = n0 + 1;
+    if (OBS & 1) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            a.obs_pop[(long long)q * a.ld + n0] = (double)s[q].x + L::w(q);
+            if (live1) a.obs_pop[(long long)q * a.ld + n1] = (double)s[q].y + L::w(q);
+        }
+    }
+    if ((m0 >> Meta<Q>::NW_SHIFT) & 1) {
+        const int k = a.aux[n0];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) a.nw_s[(long long)q * a.n_nw + k] = s[q].x;
+    }
+    if ((m1 >> Meta<Q>::NW_SHIFT) & 1) {
+        const int k = a.aux[n1];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) a.nw_s[(long long)q * a.n_nw + k] = s[q].y;
+    }
+    float2 drho, u[3];
+    collide_pair<Q>(s, (float)a.omega, drho, u);
+    if (!isfinite(drho.x) || (live1 && !isfinite(drho.y))) atomicOr(a.flags, FLAG_NONFINITE);
+    if (OBS & 2) {
+        a.obs_mom[n0] = 1.0 + (double)drho.x;
+        a.obs_mom[a.ld + n0] = (double)u[0].x;
+        a.obs_mom[2 * a.ld + n0] = (double)u[1].x;
+        a.obs_mom[3 * a.ld + n0] = (double)u[2].x;
+        if (live1) {
+            a.obs_mom[n1] = 1.0 + (double)drho.y;
+            a.obs_mom[a.ld + n1] = (double)u[0].y;
+            a.obs_mom[2 * a.ld + n1] = (double)u[1].y;
+            a.obs_mom[3 * a.ld + n1] = (double)u[2].y;
+        }
+    }
+    // the open-boundary pass needs the outlet nodes' collision velocity
+    if ((int)((m0 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_OUTLET) {
+        double* o = a.io_u + 3 * (long long)a.aux[n0];
+        o[0] = (double)u[0].x;
+        o[1] = (double)u[1].x;
+        o[2] = (double)u[2].x;
+    }
+    if ((int)((m1 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_OUTLET) {
+        double* o = a.io_u + 3 * (long long)a.aux[n1];
+        o[0] = (double)u[0].y;
+        o[1] = (double)u[1].y;
+        o[2] = (double)u[2].y;
+    }
+}
+
+// Phase-1 gather of a pair: each node from its upstream neighbours' slots,
+// or its own opposite slot where the upstream node is missing (a padding
+// node has m = 0 and reads its own padding slots).
+template <class S, int Q>
+__device__ __forceinline__ void pair_gather1(const StepArgs<S, Q>& a, float2 s[Q], typename Meta<Q>::T m0,
+                                             typename Meta<Q>::T m1, const int* sd0, const int* sd1, int n0) {
+    using L = Lat<Q>;
+    using IO = PairIO<S>;
+    // element indices fit 32 bits (the launcher requires Q * ld < 2^32)
+    const unsigned ld = (unsigned)a.ld, u0 = (unsigned)n0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (q == L::REST) {
+            s[q] = IO::get2(a.pop + (q * ld + u0));
+        } else {
+            const int oq = L::opp(q);
+            const unsigned own0 = q * ld + u0;
+            const unsigned i0 = ((m0 >> oq) & 1) ? oq * ld + (unsigned)(n0 + sd0[oq]) : own0;
+            const unsigned i1 = ((m1 >> oq) & 1) ? oq * ld + (unsigned)(n0 + 1 + sd1[oq]) : own0 + 1;
+            s[q] = make_float2(IO::get(a.pop + i0), IO::get(a.pop + i1));
+        }
+    }
+}
+
+// Phase-1 scatter: to the downstream neighbours' slots, or bounced back into
+// the node's own opposite slot where the neighbour is missing.
+template <class S, int Q>
+__device__ __forceinline__ void pair_scatter1(const StepArgs<S, Q>& a, const float2 s[Q], typename Meta<Q>::T m0,
+                                              typename Meta<Q>::T m1, const int* sd0, const int* sd1, int n0) {
+    using L = Lat<Q>;
+    using IO = PairIO<S>;
+    const unsigned ld = (unsigned)a.ld, u0 = (unsigned)n0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (q == L::REST) {
+            IO::put2(a.pop + (q * ld + u0), s[q]);
+            continue;
+        }
+        const int oq = L::opp(q);
+        const unsigned own0 = oq * ld + u0;
+        const unsigned i0 = ((m0 >> q) & 1) ? q * ld + (unsigned)(n0 + sd0[q]) : own0;
+        const unsigned i1 = ((m1 >> q) & 1) ? q * ld + (unsigned)(n0 + 1 + sd1[q]) : own0 + 1;
+        IO::put(a.pop + i0, s[q].x);
+        IO::put(a.pop + i1, s[q].y);
+    }
+}
+
+// Phase 0 (local slots only), one pair per thread.
+template <class S, int Q, int OBS>
+__global__ void __launch_bounds__(PAIR_THREADS, 4) pair_phase0_kernel(StepArgs<S, Q> a) {
+    using L = Lat<Q>;
+    using MT = typename Meta<Q>::T;
+    using IO = PairIO<S>;
+    const int n0 = blockIdx.x * BLOCK_NODES + 2 * threadIdx.x;
+    if (n0 >= a.n) return;
+    const bool live1 = n0 + 1 < a.n;
+    const MT m0 = a.meta[n0];
+    const MT m1 = live1 ? a.meta[n0 + 1] : MT(0);
+    float2 s[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s[q] = IO::get2(a.pop + (q * (unsigned)a.ld + (unsigned)n0));
+    pair_middle<S, Q, OBS>(a, s, m0, m1, n0, live1);
+    // a dead second node writes only its own padding slot
+#pragma unroll
+    for (int q = 0; q < Q; ++q) IO::put2(a.pop + (L::opp(q) * (unsigned)a.ld + (unsigned)n0), s[q]);
+}
+
+// ----------------------------------------------- phase 1, persistent form ---
+// The phase-1 gather depends on two metadata loads (the node's word, then its
+// segment's offsets) before the population loads can start. This form hides
+// them: each CTA walks tiles of BLOCK_NODES nodes (tile, tile + gridDim.x,
+// ...) and, while it gathers, collides and scatters one tile, copies the next
+// tile's node words and segment offsets into the other half of a
+// double-buffered shared-memory area with cp.async (global -> shared, no
+// registers held). One __syncthreads per tile hands the buffers over.
+
+__device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Resident CTAs per SM the phase-1 kernel is compiled for (caps its
+// registers: 5 x 128 threads -> 96 registers, no spills for D3Q19).
+#ifndef LBM_PAIR1_MIN_BLOCKS
+#define LBM_PAIR1_MIN_BLOCKS 5
+#endif
+
+// Bytes of one metadata buffer: the tile's node words, then its segment rows
+// (seg_smem_bytes), rounded up to 16.
+template <int Q>
+__host__ __device__ __forceinline__ int pair_buffer_bytes(int seg_smem_bytes) {
+    const int b = BLOCK_NODES * (int)sizeof(typename Meta<Q>::T) + seg_smem_bytes;
+    return (b + 15) & ~15;
+}
+
+template <class S, int Q, int OBS>
+__global__ void __launch_bounds__(PAIR_THREADS, LBM_PAIR1_MIN_BLOCKS) pair_phase1_kernel(StepArgs<S, Q> a, int n_tiles) {
+    using MT = typename Meta<Q>::T;
+    extern __shared__ __align__(16) unsigned char pair_smem[];
+    const int tid = threadIdx.x;
+    const int buf_bytes = pair_buffer_bytes<Q>(a.seg_smem_bytes);
+    auto meta_buf = [&](int b) { return reinterpret_cast<MT*>(pair_smem + b * buf_bytes); };
+    auto rows_buf = [&](int b) {
+        return reinterpret_cast<int*>(pair_smem + b * buf_bytes + BLOCK_NODES * (int)sizeof(MT));
+    };
+    auto prefetch = [&](int tile, int b) {
+        // node words: the thread's two nodes (8 or 16 bytes, aligned: n even)
+        const MT* src = a.meta + (long long)tile * BLOCK_NODES + 2 * tid;
+        if (sizeof(MT) == 4) cp_async_8(meta_buf(b) + 2 * tid, src);
+        else cp_async_16(meta_buf(b) + 2 * tid, src);
+        const int s0 = __ldg(a.seg_base + tile);
+        const int cnt = (__ldg(a.seg_base + tile + 1) - s0) * Q;
+        const int* rows = a.seg_delta + (long long)s0 * Q;
+        int* dst = rows_buf(b);
+        for (int i = tid; i < cnt; i += PAIR_THREADS) cp_async_4(dst + i, rows + i);
+        cp_async_commit();
+    };
+
+    int tile = blockIdx.x;
+    if (tile >= n_tiles) return;
+    int b = 0;
+    prefetch(tile, 0);
+    cp_async_wait_all();
+    __syncthreads();
+    for (;;) {
+        const int next = tile + gridDim.x;
+        const int n0 = tile * BLOCK_NODES + 2 * tid;
+        const bool live0 = n0 < a.n, live1 = n0 + 1 < a.n;
+        const MT m0 = meta_buf(b)[2 * tid];
+        const MT m1 = meta_buf(b)[2 * tid + 1];
+        const int* sd0 = rows_buf(b) + Q * (int)(m0 >> Meta<Q>::SEG_SHIFT);
+        const int* sd1 = rows_buf(b) + Q * (int)(m1 >> Meta<Q>::SEG_SHIFT);
+        float2 s[Q];
+        pair_gather1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
+        if (next < n_tiles) prefetch(next, b ^ 1);
+        if (live0) {
+            pair_middle<S, Q, OBS>(a, s, m0, m1, n0, live1);
+            pair_scatter1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
+        }
+        if (next >= n_tiles) break;
+        cp_async_wait_all();
+        __syncthreads();
+        tile = next;
+        b ^= 1;
+    }
+}
+
+}  // namespace lbm

@@ -59,6 +59,19 @@ struct PairIO<__nv_bfloat16> {
 
 constexpr int PAIR_THREADS = BLOCK_NODES / 2;
 
+// Resident CTAs per SM the phase-0 kernel is compiled for (caps registers).
+// Its loads carry no dependency, so occupancy is what keeps bytes in flight:
+// 6 CTAs (80 registers) for FP32, 8 (64 registers) for the 16-bit types,
+// whose 2-wide loads move half the bytes per instruction.
+template <class S>
+constexpr int pair0_min_blocks() {
+#ifdef LBM_PAIR0_MIN_BLOCKS
+    return LBM_PAIR0_MIN_BLOCKS;
+#else
+    return sizeof(S) == 4 ? 6 : 8;
+#endif
+}
+
 // BGK collision of two nodes' deviations d (in place): c = (1 - omega) d +
 // omega deq, deq_q = w_q (drho + (1 + drho)(3 c.u + 4.5 (c.u)^2 - 1.5 u^2)).
 // Returns drho and u of the input.
@@ -217,9 +230,50 @@ __device__ __forceinline__ void pair_scatter1(const StepArgs<S, Q>& a, const flo
     }
 }
 
+// The same gather and scatter for a pair whose two nodes share a segment row
+// and a neighbour mask: node n + 1's slot is node n's plus one.
+template <class S, int Q>
+__device__ __forceinline__ void pair_gather1_twin(const StepArgs<S, Q>& a, float2 s[Q], typename Meta<Q>::T m,
+                                                  const int* sd, int n0) {
+    using L = Lat<Q>;
+    using IO = PairIO<S>;
+    const unsigned ld = (unsigned)a.ld, u0 = (unsigned)n0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (q == L::REST) {
+            s[q] = IO::get2(a.pop + (q * ld + u0));
+        } else {
+            const int oq = L::opp(q);
+            const unsigned i = ((m >> oq) & 1) ? oq * ld + (unsigned)(n0 + sd[oq]) : q * ld + u0;
+            const S* p = a.pop + i;
+            s[q] = make_float2(IO::get(p), IO::get(p + 1));
+        }
+    }
+}
+
+template <class S, int Q>
+__device__ __forceinline__ void pair_scatter1_twin(const StepArgs<S, Q>& a, const float2 s[Q],
+                                                   typename Meta<Q>::T m, const int* sd, int n0) {
+    using L = Lat<Q>;
+    using IO = PairIO<S>;
+    const unsigned ld = (unsigned)a.ld, u0 = (unsigned)n0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (q == L::REST) {
+            IO::put2(a.pop + (q * ld + u0), s[q]);
+            continue;
+        }
+        const int oq = L::opp(q);
+        const unsigned i = ((m >> q) & 1) ? q * ld + (unsigned)(n0 + sd[q]) : oq * ld + u0;
+        S* p = a.pop + i;
+        IO::put(p, s[q].x);
+        IO::put(p + 1, s[q].y);
+    }
+}
+
 // Phase 0 (local slots only), one pair per thread.
 template <class S, int Q, int OBS>
-__global__ void __launch_bounds__(PAIR_THREADS, 4) pair_phase0_kernel(StepArgs<S, Q> a) {
+__global__ void __launch_bounds__(PAIR_THREADS, pair0_min_blocks<S>()) pair_phase0_kernel(StepArgs<S, Q> a) {
     using L = Lat<Q>;
     using MT = typename Meta<Q>::T;
     using IO = PairIO<S>;
@@ -262,10 +316,16 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Resident CTAs per SM the phase-1 kernel is compiled for (caps its
-// registers: 5 x 128 threads -> 96 registers, no spills for D3Q19).
-#ifndef LBM_PAIR1_MIN_BLOCKS
-#define LBM_PAIR1_MIN_BLOCKS 5
+// registers): 5 (96 registers, no spills for D3Q19) for FP32, 6 (80) for the
+// 16-bit types, measured best on the 21.4M-node vessel.
+template <class S>
+constexpr int pair1_min_blocks() {
+#ifdef LBM_PAIR1_MIN_BLOCKS
+    return LBM_PAIR1_MIN_BLOCKS;
+#else
+    return sizeof(S) == 4 ? 5 : 6;
 #endif
+}
 
 // Bytes of one metadata buffer: the tile's node words, then its segment rows
 // (seg_smem_bytes), rounded up to 16.
@@ -276,7 +336,7 @@ __host__ __device__ __forceinline__ int pair_buffer_bytes(int seg_smem_bytes) {
 }
 
 template <class S, int Q, int OBS>
-__global__ void __launch_bounds__(PAIR_THREADS, LBM_PAIR1_MIN_BLOCKS) pair_phase1_kernel(StepArgs<S, Q> a, int n_tiles) {
+__global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S>()) pair_phase1_kernel(StepArgs<S, Q> a, int n_tiles) {
     using MT = typename Meta<Q>::T;
     extern __shared__ __align__(16) unsigned char pair_smem[];
     const int tid = threadIdx.x;
@@ -312,12 +372,19 @@ __global__ void __launch_bounds__(PAIR_THREADS, LBM_PAIR1_MIN_BLOCKS) pair_phase
         const MT m1 = meta_buf(b)[2 * tid + 1];
         const int* sd0 = rows_buf(b) + Q * (int)(m0 >> Meta<Q>::SEG_SHIFT);
         const int* sd1 = rows_buf(b) + Q * (int)(m1 >> Meta<Q>::SEG_SHIFT);
+        // warps whose every pair shares one segment row and one neighbour
+        // mask address each direction once for both nodes
+        const bool twin = ((m0 ^ m1) & Meta<Q>::mask_all()) == 0 &&
+                          (m0 >> Meta<Q>::SEG_SHIFT) == (m1 >> Meta<Q>::SEG_SHIFT);
+        const bool uniform = __all_sync(0xffffffffu, twin);
         float2 s[Q];
-        pair_gather1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
+        if (uniform) pair_gather1_twin<S, Q>(a, s, m0, sd0, n0);
+        else pair_gather1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
         if (next < n_tiles) prefetch(next, b ^ 1);
         if (live0) {
             pair_middle<S, Q, OBS>(a, s, m0, m1, n0, live1);
-            pair_scatter1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
+            if (uniform) pair_scatter1_twin<S, Q>(a, s, m0, sd0, n0);
+            else pair_scatter1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
         }
         if (next >= n_tiles) break;
         cp_async_wait_all();

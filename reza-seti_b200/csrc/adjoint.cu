@@ -34,8 +34,11 @@
 #include <algorithm>
 #include <cmath>
 
+#include <type_traits>
+
 #include "adjoint.h"
 #include "lattice.cuh"
+#include "pair.cuh"
 
 namespace lbm {
 namespace {
@@ -144,17 +147,24 @@ __device__ __forceinline__ void traction_adjoint(const double tau[3], const doub
     }
 }
 
-// Sum over the block (blockDim.x a multiple of 32, at most 32 warps); the
-// result is valid in thread 0.
-__device__ __forceinline__ double block_sum(double v, double* red) {
+// FP64 sums without block barriers: each warp adds its total to one of
+// N_PARTIALS slots (spread to avoid contention on one address); the host adds
+// the slots at the end of the run.
+constexpr int N_PARTIALS = 1024;
+
+// Sum over the warp, valid in every lane (all 32 lanes active).
+__device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-    return s;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void warp_accumulate(double v, double* partials) {
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) {
+        const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        atomicAdd(partials + (w & (N_PARTIALS - 1)), v);
+    }
 }
 
 // d = f - w, rounded to R
@@ -234,38 +244,46 @@ struct ObjArgs {
     double* J;
 };
 
-// Objective term of step t at the target nodes (forward sweep): records the
-// moments of f^t and adds |tau^t|^2 / T for t >= 1.
+// Objective term of step t at the target nodes (forward sweep), one warp per
+// target and one lane per direction: records the moments of f^t and adds
+// |tau^t|^2 / T for t >= 1.
 template <class R, int Q>
 __global__ void adj_objective_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, int t) {
-    __shared__ double red[4];
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    using L = Lat<Q>;
+    const int lane = threadIdx.x & 31;
+    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     double jl = 0.0;
-    if (k < a.n_target) {
+    if (k < a.n_target) {  // uniform over the warp
         const int n = a.node[k];
-        R d[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) d[q] = D[(long long)q * a.ld + n];
-        R drho, u[3];
-        dmoments<R, Q>(d, drho, u);
+        const bool on = lane < Q;
+        const int q = on ? lane : 0;
+        const R dq = on ? D[(long long)q * a.ld + n] : R(0);
+        const double c0 = on ? L::cx(q) : 0, c1 = on ? L::cy(q) : 0, c2 = on ? L::cz(q) : 0;
+        const double drho = warp_sum((double)dq);
+        const double rho = 1.0 + drho;
+        const double u0 = warp_sum(c0 * (double)dq) / rho, u1 = warp_sum(c1 * (double)dq) / rho,
+                     u2 = warp_sum(c2 * (double)dq) / rho;
         double* mt = a.mom + ((long long)t * a.n_target + k) * 4;
         if (t >= 1) {
             const double* mp = mt - 4 * (long long)a.n_target;
             const R up[3] = {(R)mp[1], (R)mp[2], (R)mp[3]};
-            R fne[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) fne[q] = d[q] - deq<R, Q>(q, (R)mp[0], up);
-            double tau[3];
-            traction<Q>(fne, a.nw_normal + 3 * (long long)a.nw[k], a.cw, tau);
-            jl = a.inv_T * (tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
+            const double fne = on ? (double)(dq - deq<R, Q>(q, (R)mp[0], up)) : 0.0;
+            const double* nrm = a.nw_normal + 3 * (long long)a.nw[k];
+            const double cn = c0 * nrm[0] + c1 * nrm[1] + c2 * nrm[2];
+            const double f = fne * cn;
+            const double t0 = a.cw * warp_sum(f * (c0 - cn * nrm[0]));
+            const double t1 = a.cw * warp_sum(f * (c1 - cn * nrm[1]));
+            const double t2 = a.cw * warp_sum(f * (c2 - cn * nrm[2]));
+            if (lane == 0) jl = a.inv_T * (t0 * t0 + t1 * t1 + t2 * t2);
         }
-        mt[0] = (double)drho;
-        mt[1] = (double)u[0];
-        mt[2] = (double)u[1];
-        mt[3] = (double)u[2];
+        if (lane == 0) {
+            mt[0] = drho;
+            mt[1] = u0;
+            mt[2] = u1;
+            mt[3] = u2;
+        }
     }
-    const double s = block_sum(jl, red);
-    if (threadIdx.x == 0 && s != 0.0) atomicAdd(a.J, s);
+    warp_accumulate(jl, a.J);
 }
 
 // lambda^t from lambda^{t+1} at every node (the transpose of the push). One
@@ -278,7 +296,6 @@ __global__ void __launch_bounds__(AT) adj_pull_kernel(AGeom<R, Q> g, const R* __
                                                        const R* __restrict__ Ln, R* __restrict__ Lc, double s_t,
                                                        double* __restrict__ dspeed, double* __restrict__ domega) {
     using L = Lat<Q>;
-    __shared__ double red[AT / 32];
     const int n = blockIdx.x * AT + threadIdx.x;
     double wl = 0.0;
     if (n < g.n) {
@@ -352,52 +369,359 @@ __global__ void __launch_bounds__(AT) adj_pull_kernel(AGeom<R, Q> g, const R* __
         wl = (double)(mueq - mud);
         if (kind == KIND_INLET) dspeed[g.aux[n]] += (double)gin * s_t;
     }
-    const double s = block_sum(wl, red);
-    if (threadIdx.x == 0 && s != 0.0) atomicAdd(domega, s);
+    warp_accumulate(wl, domega);
 }
 
-// Objective terms of lambda^t at the target nodes: dJ_t/df^t (t >= 1) and
-// dJ_{t+1}/df^t through the f_eq of tau^{t+1} (t < T).
+// Objective terms of lambda^t at the target nodes, one warp per target and
+// one lane per direction: dJ_t/df^t (t >= 1) and dJ_{t+1}/df^t through the
+// f_eq of tau^{t+1} (t < T).
 template <class R, int Q>
 __global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, const R* __restrict__ Dn,
                                              R* __restrict__ Lc, int t, int T) {
     using L = Lat<Q>;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a.n_target) return;
+    const int lane = threadIdx.x & 31;
+    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (k >= a.n_target) return;  // uniform over the warp
     const int n = a.node[k];
+    const bool on = lane < Q;
+    const int q = on ? lane : 0;
+    const double c0 = on ? L::cx(q) : 0, c1 = on ? L::cy(q) : 0, c2 = on ? L::cz(q) : 0;
     const double* nrm = a.nw_normal + 3 * (long long)a.nw[k];
+    const double cn = c0 * nrm[0] + c1 * nrm[1] + c2 * nrm[2];
+    const double m0 = c0 - cn * nrm[0], m1 = c1 - cn * nrm[1], m2 = c2 - cn * nrm[2];
     const double scale = 2.0 * a.inv_T * a.cw;
-    R acc[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) acc[q] = R(0);
+    double g = 0.0;
     if (t >= 1) {
         const double* mp = a.mom + ((long long)(t - 1) * a.n_target + k) * 4;
         const R up[3] = {(R)mp[1], (R)mp[2], (R)mp[3]};
-        R fne[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) fne[q] = D[(long long)q * a.ld + n] - deq<R, Q>(q, (R)mp[0], up);
-        double tau[3];
-        traction<Q>(fne, nrm, a.cw, tau);
-        traction_adjoint<Q>(tau, nrm, scale, acc);
+        const double fne = on ? (double)(D[(long long)q * a.ld + n] - deq<R, Q>(q, (R)mp[0], up)) : 0.0;
+        const double f = fne * cn;
+        const double t0 = a.cw * warp_sum(f * m0), t1 = a.cw * warp_sum(f * m1), t2 = a.cw * warp_sum(f * m2);
+        g = scale * cn * (t0 * m0 + t1 * m1 + t2 * m2);
     }
     if (t < T) {
         const double* mt = a.mom + ((long long)t * a.n_target + k) * 4;
         const R ut[3] = {(R)mt[1], (R)mt[2], (R)mt[3]};
-        R fne[Q];
+        const double fne = on ? (double)(Dn[(long long)q * a.ld + n] - deq<R, Q>(q, (R)mt[0], ut)) : 0.0;
+        const double f = fne * cn;
+        const double t0 = a.cw * warp_sum(f * m0), t1 = a.cw * warp_sum(f * m1), t2 = a.cw * warp_sum(f * m2);
+        const double gq = on ? scale * cn * (t0 * m0 + t1 * m1 + t2 * m2) : 0.0;
+        // sum_r gq_r d feq_r / d f_q = A + B . c_q at the moments of f^t
+        const double u[3] = {mt[1], mt[2], mt[3]};
+        const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        const double cu = c0 * u[0] + c1 * u[1] + c2 * u[2];
+        const double gw = gq * (on ? L::w(q) : 0.0);
+        const double A = warp_sum(gw * (1.0 - 4.5 * cu * cu + 1.5 * usq));
+        const double kk = 3.0 + 9.0 * cu;
+        const double B0 = warp_sum(gw * (kk * c0 - 3.0 * u[0]));
+        const double B1 = warp_sum(gw * (kk * c1 - 3.0 * u[1]));
+        const double B2 = warp_sum(gw * (kk * c2 - 3.0 * u[2]));
+        g -= A + B0 * c0 + B1 * c1 + B2 * c2;
+    }
+    if (on) Lc[(long long)q * a.ld + n] += (R)g;
+}
+
+// ------------------------------------------------ FP32 kernels, node pairs ---
+// FP32 forms of the push and pull kernels over two adjacent nodes per thread
+// (the engine's pair layout, n even): 2-wide coalesced access to the nodes'
+// own slots, packed FP32 arithmetic (the engine's collide_pair for the
+// forward collision), and one address per direction for both nodes of a
+// "twin" pair (same segment row and neighbour mask, neither node on an open
+// boundary). Other pairs take each node through the scalar rules. Slot
+// indices are 32-bit (the launcher requires Q * ld < 2^32).
+
+template <int Q>
+__device__ __forceinline__ bool adj_open(typename Meta<Q>::T m) {
+    const int k = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    return k == KIND_INLET || k == KIND_OUTLET;
+}
+
+template <int Q>
+__device__ __forceinline__ bool adj_twin(typename Meta<Q>::T m0, typename Meta<Q>::T m1) {
+    return ((m0 ^ m1) & Meta<Q>::mask_all()) == 0 && (m0 >> Meta<Q>::SEG_SHIFT) == (m1 >> Meta<Q>::SEG_SHIFT) &&
+           !adj_open<Q>(m0) && !adj_open<Q>(m1);
+}
+
+// c_q . v for two nodes, from adds and subtractions
+template <int Q>
+__device__ __forceinline__ float2 cdot2(int q, const float2 v[3]) {
+    using L = Lat<Q>;
+    float2 r = f2s(0.f);
+    bool first = true;
+    const int c[3] = {L::cx(q), L::cy(q), L::cz(q)};
 #pragma unroll
-        for (int q = 0; q < Q; ++q) fne[q] = Dn[(long long)q * a.ld + n] - deq<R, Q>(q, (R)mt[0], ut);
-        double tau[3];
-        traction<Q>(fne, nrm, a.cw, tau);
-        R gq[Q];
-        traction_adjoint<Q>(tau, nrm, scale, gq);
-        R A, B[3];
-        feq_adjoint<R, Q>(gq, ut, A, B);
+    for (int k = 0; k < 3; ++k) {
+        if (!c[k]) continue;
+        if (first) {
+            r = c[k] > 0 ? v[k] : f2mul(f2s(-1.f), v[k]);
+            first = false;
+        } else {
+            r = c[k] > 0 ? f2add(r, v[k]) : f2sub(r, v[k]);
+        }
+    }
+    return r;
+}
+
+// One node's push scatter with the open-boundary corrections (scalar rules).
+template <int Q>
+__device__ __forceinline__ void push_scatter_node(const AGeom<float, Q>& g, float* __restrict__ Dn, int n,
+                                                  typename Meta<Q>::T m, const int* sd, const float c[Q],
+                                                  const float u[3], double s_t) {
+    using L = Lat<Q>;
+    const unsigned ld = (unsigned)g.ld, un = (unsigned)n;
+    const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    float nrm[3] = {0.f, 0.f, 0.f};
+    float vin = 0.f;
+    if (kind == KIND_INLET) {
+        for (int k = 0; k < 3; ++k) nrm[k] = (float)g.in_normal[k];
+        vin = (float)(g.speed[g.aux[n]] * s_t);
+    } else if (kind == KIND_OUTLET) {
+        for (int k = 0; k < 3; ++k) nrm[k] = g.out_nrm[3 * (long long)g.aux[n] + k];
+    }
+    const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
 #pragma unroll
-        for (int q = 0; q < Q; ++q)
-            acc[q] -= A + R(L::cx(q)) * B[0] + R(L::cy(q)) * B[1] + R(L::cz(q)) * B[2];
+    for (int q = 0; q < Q; ++q) {
+        if (q == L::REST) {
+            Dn[q * ld + un] = c[q];
+        } else if ((m >> q) & 1) {
+            Dn[q * ld + (unsigned)(n + sd[q])] = c[q];
+        } else {
+            float v = c[q];
+            const float cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
+            if (cn > 0.f) {
+                if (kind == KIND_INLET) {
+                    v = c[q] + (float)(6.0 * L::w(q)) * cn * vin;
+                } else {
+                    const float cu = L::cx(q) * u[0] + L::cy(q) * u[1] + L::cz(q) * u[2];
+                    const float eq = 1.f + 4.5f * cu * cu - 1.5f * usq;
+                    v = -c[q] + (float)(2.0 * L::w(q)) * ((float)g.out_rho * eq - 1.f);
+                }
+            }
+            Dn[L::opp(q) * ld + un] = v;
+        }
+    }
+}
+
+template <int Q>
+__global__ void __launch_bounds__(PAIR_THREADS, 6)
+    adj_push_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t) {
+    using L = Lat<Q>;
+    using MT = typename Meta<Q>::T;
+    const int n0 = blockIdx.x * BLOCK_NODES + 2 * threadIdx.x;
+    if (n0 >= g.n) return;
+    const bool live1 = n0 + 1 < g.n;
+    const MT m0 = g.meta[n0];
+    const MT m1 = live1 ? g.meta[n0 + 1] : MT(0);
+    const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
+    float2 s[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s[q] = *reinterpret_cast<const float2*>(D + (q * ld + u0));
+    float2 drho, u[3];
+    collide_pair<Q>(s, g.omega, drho, u);
+    const int* sd0 = nbr_row<Q>(g.seg_base, g.seg_delta, n0, m0);
+    if (adj_twin<Q>(m0, m1)) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (q == L::REST) {
+                *reinterpret_cast<float2*>(Dn + (q * ld + u0)) = s[q];
+                continue;
+            }
+            const unsigned i = ((m0 >> q) & 1) ? q * ld + (unsigned)(n0 + sd0[q]) : L::opp(q) * ld + u0;
+            Dn[i] = s[q].x;
+            Dn[i + 1] = s[q].y;
+        }
+    } else {
+        float c[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) c[q] = s[q].x;
+        const float ux[3] = {u[0].x, u[1].x, u[2].x};
+        push_scatter_node<Q>(g, Dn, n0, m0, sd0, c, ux, s_t);
+        if (live1) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) c[q] = s[q].y;
+            const float uy[3] = {u[0].y, u[1].y, u[2].y};
+            push_scatter_node<Q>(g, Dn, n0 + 1, m1, nbr_row<Q>(g.seg_base, g.seg_delta, n0 + 1, m1), c, uy, s_t);
+        }
+    }
+}
+
+// One node's pull gather (scalar rules): mu_q, the inlet-speed sensitivity
+// factor and the set of outlet links.
+template <int Q>
+__device__ __forceinline__ void pull_gather_node(const AGeom<float, Q>& g, const float* __restrict__ Ln, int n,
+                                                 typename Meta<Q>::T m, const int* sd, float mu[Q], float& gin,
+                                                 unsigned& out_links) {
+    using L = Lat<Q>;
+    const unsigned ld = (unsigned)g.ld, un = (unsigned)n;
+    const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    float nrm[3] = {0.f, 0.f, 0.f};
+    if (kind == KIND_INLET) {
+        for (int k = 0; k < 3; ++k) nrm[k] = (float)g.in_normal[k];
+    } else if (kind == KIND_OUTLET) {
+        for (int k = 0; k < 3; ++k) nrm[k] = g.out_nrm[3 * (long long)g.aux[n] + k];
     }
 #pragma unroll
-    for (int q = 0; q < Q; ++q) Lc[(long long)q * a.ld + n] += acc[q];
+    for (int q = 0; q < Q; ++q) {
+        float v;
+        if (q == L::REST) {
+            v = Ln[q * ld + un];
+        } else if ((m >> q) & 1) {
+            v = Ln[q * ld + (unsigned)(n + sd[q])];
+        } else {
+            v = Ln[L::opp(q) * ld + un];
+            const float cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
+            if (cn > 0.f) {
+                if (kind == KIND_INLET) {
+                    gin += v * (float)(6.0 * L::w(q)) * cn;
+                } else {
+                    v = -v;
+                    out_links |= 1u << q;
+                }
+            }
+        }
+        mu[q] = v;
+    }
+}
+
+template <int Q>
+__global__ void __launch_bounds__(PAIR_THREADS, 4)
+    adj_pull_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
+                         float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
+                         double* __restrict__ domega) {
+    using L = Lat<Q>;
+    using MT = typename Meta<Q>::T;
+    const int n0 = blockIdx.x * BLOCK_NODES + 2 * threadIdx.x;
+    double wl = 0.0;
+    if (n0 < g.n) {
+        const bool live1 = n0 + 1 < g.n;
+        const MT m0 = g.meta[n0];
+        const MT m1 = live1 ? g.meta[n0 + 1] : MT(0);
+        const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
+        const int* sd0 = nbr_row<Q>(g.seg_base, g.seg_delta, n0, m0);
+        float2 mu[Q];
+        float gin0 = 0.f, gin1 = 0.f;
+        unsigned ol0 = 0, ol1 = 0;
+        if (adj_twin<Q>(m0, m1)) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                if (q == L::REST) {
+                    mu[q] = *reinterpret_cast<const float2*>(Ln + (q * ld + u0));
+                } else {
+                    const unsigned i = ((m0 >> q) & 1) ? q * ld + (unsigned)(n0 + sd0[q]) : L::opp(q) * ld + u0;
+                    mu[q] = make_float2(Ln[i], Ln[i + 1]);
+                }
+            }
+        } else {
+            float t[Q];
+            pull_gather_node<Q>(g, Ln, n0, m0, sd0, t, gin0, ol0);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) mu[q].x = t[q];
+            if (live1) {
+                pull_gather_node<Q>(g, Ln, n0 + 1, m1, nbr_row<Q>(g.seg_base, g.seg_delta, n0 + 1, m1), t, gin1,
+                                    ol1);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) mu[q].y = t[q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) mu[q].y = 0.f;
+            }
+        }
+        // moments of f^t and sum mu d, streaming the node's own slots
+        float2 ra = f2s(0.f), rb = f2s(0.f), j0 = f2s(0.f), j1 = f2s(0.f), j2 = f2s(0.f), mud = f2s(0.f);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float2 dq = *reinterpret_cast<const float2*>(D + (q * ld + u0));
+            if (q & 1) rb = f2add(rb, dq);
+            else ra = f2add(ra, dq);
+            if (L::cx(q)) j0 = L::cx(q) > 0 ? f2add(j0, dq) : f2sub(j0, dq);
+            if (L::cy(q)) j1 = L::cy(q) > 0 ? f2add(j1, dq) : f2sub(j1, dq);
+            if (L::cz(q)) j2 = L::cz(q) > 0 ? f2add(j2, dq) : f2sub(j2, dq);
+            mud = f2fma(mu[q], dq, mud);
+        }
+        const float2 drho = f2add(ra, rb);
+        const float2 rho = f2add(f2s(1.f), drho);
+        const float2 irho = make_float2(1.f / rho.x, 1.f / rho.y);
+        const float2 u[3] = {f2mul(j0, irho), f2mul(j1, irho), f2mul(j2, irho)};
+        const float2 usq = f2fma(u[0], u[0], f2fma(u[1], u[1], f2mul(u[2], u[2])));
+        // outlet links: d/du of 2 w rho_out eq(u), times lambda = -mu (scalar, rare)
+        float2 G[3] = {f2s(0.f), f2s(0.f), f2s(0.f)};
+        if (ol0 | ol1) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const float c0 = (float)L::cx(q), c1 = (float)L::cy(q), c2 = (float)L::cz(q);
+                const float k2 = (float)(2.0 * L::w(q) * g.out_rho);
+                if ((ol0 >> q) & 1) {
+                    const float cu = c0 * u[0].x + c1 * u[1].x + c2 * u[2].x;
+                    const float k = -mu[q].x * k2;
+                    G[0].x += k * (9.f * cu * c0 - 3.f * u[0].x);
+                    G[1].x += k * (9.f * cu * c1 - 3.f * u[1].x);
+                    G[2].x += k * (9.f * cu * c2 - 3.f * u[2].x);
+                }
+                if ((ol1 >> q) & 1) {
+                    const float cu = c0 * u[0].y + c1 * u[1].y + c2 * u[2].y;
+                    const float k = -mu[q].y * k2;
+                    G[0].y += k * (9.f * cu * c0 - 3.f * u[0].y);
+                    G[1].y += k * (9.f * cu * c1 - 3.f * u[1].y);
+                    G[2].y += k * (9.f * cu * c2 - 3.f * u[2].y);
+                }
+            }
+        }
+        // A = sum mu w (1 - 4.5 cu^2 + 1.5 u^2), B = sum mu w (3 + 9 cu) c - 3 u sum mu w,
+        // sum mu deq, over direction pairs (q, opp q): cu flips sign
+        const float2 base = f2fma(rho, f2mul(f2s(-1.5f), usq), drho);
+        const float2 rho3 = f2mul(f2s(3.f), rho);
+        const float2 a0 = f2fma(f2s(1.5f), usq, f2s(1.f));
+        float2 A = f2s(0.f), Wm = f2s(0.f), mueq = f2s(0.f);
+        float2 Bc[3] = {f2s(0.f), f2s(0.f), f2s(0.f)};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int o = L::opp(q);
+            const float2 w = f2s((float)L::w(q));
+            if (q == L::REST) {
+                const float2 wm = f2mul(w, mu[q]);
+                A = f2fma(wm, a0, A);
+                Wm = f2add(Wm, wm);
+                mueq = f2fma(wm, base, mueq);
+                continue;
+            }
+            if (o < q) continue;
+            const float2 cu = cdot2<Q>(q, u);
+            const float2 mp = f2mul(w, f2add(mu[q], mu[o]));
+            const float2 mm = f2mul(w, f2sub(mu[q], mu[o]));
+            const float2 cu2 = f2mul(cu, cu);
+            A = f2fma(mp, f2fma(f2s(-4.5f), cu2, a0), A);
+            Wm = f2add(Wm, mp);
+            const float2 sym = f2fma(rho, f2mul(f2s(4.5f), cu2), base);
+            const float2 anti = f2mul(rho3, cu);
+            mueq = f2fma(sym, mp, f2fma(anti, mm, mueq));
+            // (3 mm + 9 cu mp) c
+            const float2 bk = f2fma(f2s(9.f), f2mul(cu, mp), f2mul(f2s(3.f), mm));
+            if (L::cx(q)) Bc[0] = L::cx(q) > 0 ? f2add(Bc[0], bk) : f2sub(Bc[0], bk);
+            if (L::cy(q)) Bc[1] = L::cy(q) > 0 ? f2add(Bc[1], bk) : f2sub(Bc[1], bk);
+            if (L::cz(q)) Bc[2] = L::cz(q) > 0 ? f2add(Bc[2], bk) : f2sub(Bc[2], bk);
+        }
+        const float2 B[3] = {f2fma(f2s(-3.f), f2mul(u[0], Wm), Bc[0]), f2fma(f2s(-3.f), f2mul(u[1], Wm), Bc[1]),
+                             f2fma(f2s(-3.f), f2mul(u[2], Wm), Bc[2])};
+        const float2 gu = f2fma(G[0], u[0], f2fma(G[1], u[1], f2mul(G[2], u[2])));
+        const float2 keep = f2s(1.f - g.omega), om = f2s(g.omega);
+        // lambda_q = (1 - omega) mu_q + omega (A + B.c_q) + (G.c_q - G.u) / rho
+        const float2 Ao = f2mul(om, A);
+        const float2 ngu = f2mul(f2s(-1.f), f2mul(gu, irho));
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float2 bc = cdot2<Q>(q, B);
+            const float2 gc = cdot2<Q>(q, G);
+            float2 lam = f2fma(keep, mu[q], f2fma(om, bc, Ao));
+            lam = f2add(lam, f2fma(gc, irho, ngu));
+            *reinterpret_cast<float2*>(Lc + (q * ld + u0)) = lam;
+        }
+        const float2 wq = f2sub(mueq, mud);
+        wl = (double)wq.x + (live1 ? (double)wq.y : 0.0);
+        if ((int)((m0 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET) dspeed[g.aux[n0]] += (double)gin0 * s_t;
+        if (live1 && (int)((m1 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET)
+            dspeed[g.aux[n0 + 1]] += (double)gin1 * s_t;
+    }
+    warp_accumulate(wl, domega);
 }
 
 struct Arena {
@@ -455,7 +779,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     double* mom = ar.get<double>((size_t)(T + 1) * std::max(nt, 1) * 4);
     double* speed = ar.get<double>(std::max(s.n_in, 1));
     double* dspeed = ar.get<double>(std::max(s.n_in, 1));
-    double* scal = ar.get<double>(2);
+    double* scal = ar.get<double>(2 * N_PARTIALS);  // J, then dJ/domega partial sums
     int* tnode = ar.get<int>(std::max(nt, 1));
     int* tnw = ar.get<int>(std::max(nt, 1));
     if (ar.err != cudaSuccess) {
@@ -476,7 +800,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         cudaMemcpyAsync(tnw, tw.data(), sizeof(int) * tw.size(), cudaMemcpyHostToDevice, st);
         if (s.n_in) cudaMemcpyAsync(speed, s.speed.data(), sizeof(double) * s.n_in, cudaMemcpyHostToDevice, st);
         cudaMemsetAsync(dspeed, 0, sizeof(double) * std::max(s.n_in, 1), st);
-        cudaMemsetAsync(scal, 0, 2 * sizeof(double), st);
+        cudaMemsetAsync(scal, 0, 2 * N_PARTIALS * sizeof(double), st);
         // the host vectors above die at the end of this block
         cudaError_t ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) {
@@ -508,9 +832,27 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     oa.J = scal;
 
     const dim3 grid((unsigned)((s.n + AT - 1) / AT));
-    const unsigned tgrid = (unsigned)((nt + 127) / 128);
+    const unsigned tgrid = (unsigned)((nt + 3) / 4);  // one warp per target, 4 per block
+    // FP32 runs the node-pair kernels (32-bit slot indices)
+    const bool pairs = std::is_same<R, float>::value && (long long)Q * s.ld < (1LL << 32);
+    const dim3 pgrid((unsigned)((s.n + BLOCK_NODES - 1) / BLOCK_NODES));
     auto push = [&](const R* D, R* Dn, int64_t t) {
+        if constexpr (std::is_same<R, float>::value) {
+            if (pairs) {
+                adj_push_pair_kernel<Q><<<pgrid, PAIR_THREADS, 0, st>>>(g, D, Dn, s.factors[t]);
+                return;
+            }
+        }
         adj_push_kernel<R, Q><<<grid, AT, 0, st>>>(g, D, Dn, s.factors[t]);
+    };
+    auto pull = [&](const R* D, const R* Ln, R* Lc, int64_t t) {
+        if constexpr (std::is_same<R, float>::value) {
+            if (pairs) {
+                adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, 0, st>>>(g, D, Ln, Lc, s.factors[t], dspeed, scal + N_PARTIALS);
+                return;
+            }
+        }
+        adj_pull_kernel<R, Q><<<grid, AT, 0, st>>>(g, D, Ln, Lc, s.factors[t], dspeed, scal + N_PARTIALS);
     };
     auto objective = [&](const R* D, int64_t t) {
         if (nt) adj_objective_kernel<R, Q><<<tgrid, 128, 0, st>>>(oa, D, (int)t);
@@ -568,8 +910,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
                 if (t == T) {
                     cudaMemsetAsync(Lcur, 0, field * sizeof(R), st);
                 } else {
-                    adj_pull_kernel<R, Q><<<grid, AT, 0, st>>>(g, seg[t - t0], Lnext, Lcur, s.factors[t], dspeed,
-                                                                scal + 1);
+                    pull(seg[t - t0], Lnext, Lcur, t);
                 }
                 if (nt)
                     adj_objective_adjoint_kernel<R, Q><<<tgrid, 128, 0, st>>>(
@@ -592,10 +933,14 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     }
     cudaEventElapsedTime(&o.forward_ms, ev.e[0], ev.e[1]);
     if (s.gradient) cudaEventElapsedTime(&o.reverse_ms, ev.e[1], ev.e[2]);
-    double hs[2] = {0, 0};
-    cudaMemcpy(hs, scal, sizeof(hs), cudaMemcpyDeviceToHost);
-    o.J = hs[0];
-    o.dJ_domega = hs[1];
+    std::vector<double> hs(2 * N_PARTIALS);
+    cudaMemcpy(hs.data(), scal, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost);
+    o.J = 0.0;
+    o.dJ_domega = 0.0;
+    for (int i = 0; i < N_PARTIALS; ++i) {
+        o.J += hs[i];
+        o.dJ_domega += hs[N_PARTIALS + i];
+    }
     o.dJ_dspeed.assign(s.n_in, 0.0);
     if (s.gradient && s.n_in)
         cudaMemcpy(o.dJ_dspeed.data(), dspeed, sizeof(double) * s.n_in, cudaMemcpyDeviceToHost);

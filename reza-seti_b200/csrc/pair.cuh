@@ -246,7 +246,9 @@ __device__ __forceinline__ void pair_gather1_twin(const StepArgs<S, Q>& a, float
             const int oq = L::opp(q);
             const unsigned i = ((m >> oq) & 1) ? oq * ld + (unsigned)(n0 + sd[oq]) : q * ld + u0;
             const S* p = a.pop + i;
-            s[q] = make_float2(IO::get(p), IO::get(p + 1));
+            // an even slot index is 2-wide aligned: one access for both nodes
+            if (i & 1) s[q] = make_float2(IO::get(p), IO::get(p + 1));
+            else s[q] = IO::get2(p);
         }
     }
 }
@@ -266,8 +268,12 @@ __device__ __forceinline__ void pair_scatter1_twin(const StepArgs<S, Q>& a, cons
         const int oq = L::opp(q);
         const unsigned i = ((m >> q) & 1) ? q * ld + (unsigned)(n0 + sd[q]) : oq * ld + u0;
         S* p = a.pop + i;
-        IO::put(p, s[q].x);
-        IO::put(p + 1, s[q].y);
+        if (i & 1) {
+            IO::put(p, s[q].x);
+            IO::put(p + 1, s[q].y);
+        } else {
+            IO::put2(p, s[q]);
+        }
     }
 }
 

@@ -263,6 +263,9 @@ def run_gpu(args):
     adjoint = None
     if rank == 0 and not args.no_adjoint:
         adjoint = run_adjoint(torch, device)
+    configs = None
+    if rank == 0 and not args.no_configs:
+        configs = run_configs(torch, device)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -285,7 +288,7 @@ def run_gpu(args):
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": 2 * args.steps, "clocks": clocks, "device_flags": flags,
-            "variants": variants, "precision": precision, "adjoint": adjoint,
+            "variants": variants, "precision": precision, "adjoint": adjoint, "configs": configs,
         }
         print(json.dumps(line))
     if dist:
@@ -409,6 +412,85 @@ def run_precision(torch, device, topo=None):
                         "wss_rel_l2": l2(wss, ref[2]), "velocity_rel_l2": l2(u, ref[4]),
                         "populations_rel_l2": l2(d, ref[3])})
         out[storage] = row
+    return out
+
+
+# ----------------------------------------------- branching and aneurysm ---
+CFG_PERIOD, CFG_PERIODS, CFG_MEAN = 4000, 2, 0.03
+
+
+def run_configs(torch, device):
+    """The Y-bifurcation (D3Q27, tau 0.55) and the saccular aneurysm (D3Q19,
+    tau 0.55) over two periods of a seeded 4-harmonic waveform (period 4000
+    steps, mean inflow 0.03 lu): kernel MLUPS per storage type (fluid nodes
+    and, for the aneurysm, box cells), TAWSS / OSI (FP64 accumulators), and
+    the errors of FP32 / FP16 storage against FP64 storage."""
+    from lbm_b200 import Engine
+    from lbm_b200 import geometry as G
+    amp, phase = harmonic_waveform(seed=5)
+    steps = CFG_PERIOD * CFG_PERIODS
+
+    def l2(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    def one(topo, q, storage, tau):
+        e = Engine(topo, tau=tau, dt=1e-5, spacing=1.0, lattice=q, storage=storage, device=device, bc="physics")
+        e.set_inlet_profile(G.inlet_disc_profile(topo, CFG_MEAN))
+        e.set_waveform(float(CFG_PERIOD), amp, phase)
+        e.set_flow(False, 0.0, harmonic=True)
+        e.set_observation(False)
+        ms_step, ms_bnd = e.step_timed(steps - 1)
+        e.set_observation(True)
+        e.step(1)
+        osi, tawss = e.osi_tawss()
+        u = e.macros()[1]
+        inl, outs = e.flux()
+        res = {"kernel_ms_per_step": round((ms_step + ms_bnd) / (steps - 1), 5), "device_flags": e.flags(),
+               "inlet_flux": inl, "outlet_fluxes": outs.tolist()}
+        e.close()
+        return res, osi, tawss, u, (ms_step + ms_bnd) / (steps - 1)
+
+    out = {"waveform": {"period_steps": CFG_PERIOD, "amplitude": np.round(amp, 4).tolist(),
+                        "phase": np.round(phase, 4).tolist(), "seed": 5, "mean_inlet_velocity": CFG_MEAN},
+           "steps": steps}
+    topo = G.y_bifurcation()
+    n = len(topo["kind"])
+    bif = {"workload": "Y-bifurcation, parent R=24 L=200, daughters R=18/16 L=180 at +-35 deg, box 256x256x348",
+           "lattice": "D3Q27", "tau": 0.55, "fluid_nodes": n}
+    ref = None
+    for storage in ("f64", "f32"):
+        res, osi, tawss, u, ms = one(topo, 27, storage, 0.55)
+        res["MLUPS"] = round(n / ms / 1e3, 1)
+        if ref is None:
+            ref = (osi, tawss, u)
+        else:
+            res.update({"tawss_rel_l2": l2(tawss, ref[1]), "osi_abs_max": float(np.max(np.abs(osi - ref[0]))),
+                        "velocity_rel_l2": l2(u, ref[2])})
+        bif[storage] = res
+    out["bifurcation"] = bif
+
+    topo = G.saccular_aneurysm()
+    n = len(topo["kind"])
+    cells = 1024 * 512 * 512
+    sac = G.sac_wall_targets(topo)
+    an = {"workload": "saccular aneurysm: R=20 tube, 90 deg bend of radius 120, R=40 sac on the outer wall, "
+                      "box 1024x512x512", "lattice": "D3Q19", "tau": 0.55, "fluid_nodes": n, "box_cells": cells,
+          "sac_wall_nodes": int(len(sac))}
+    ref = None
+    for storage in ("f64", "f32", "f16"):
+        res, osi, tawss, u, ms = one(topo, 19, storage, 0.55)
+        res["MLUPS"] = round(n / ms / 1e3, 1)
+        res["box_cell_MLUPS"] = round(cells / ms / 1e3, 1)
+        res["sac_tawss_mean"] = float(np.mean(tawss[sac]))
+        res["sac_osi_mean"] = float(np.mean(osi[sac]))
+        if ref is None:
+            ref = (osi, tawss, u)
+        else:
+            res.update({"sac_tawss_rel_l2": l2(tawss[sac], ref[1][sac]),
+                        "sac_osi_abs_max": float(np.max(np.abs(osi[sac] - ref[0][sac]))),
+                        "tawss_rel_l2": l2(tawss, ref[1]), "velocity_rel_l2": l2(u, ref[2])})
+        an[storage] = res
+    out["aneurysm"] = an
     return out
 
 
@@ -612,8 +694,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--section", default="all", choices=["all", "precision", "adjoint"],
-                    help="run only the precision study or only the adjoint measurement")
+    ap.add_argument("--no-configs", action="store_true")
+    ap.add_argument("--section", default="all", choices=["all", "precision", "adjoint", "configs"],
+                    help="run only the precision study, the adjoint measurement or the branching/aneurysm runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -622,7 +705,8 @@ def main():
     elif args.section != "all":
         import torch
         torch.cuda.set_device(0)
-        res = run_precision(torch, 0) if args.section == "precision" else run_adjoint(torch, 0)
+        run = {"precision": run_precision, "adjoint": run_adjoint, "configs": run_configs}[args.section]
+        res = run(torch, 0)
         print(json.dumps({"section": args.section, **res}))
     else:
         run_gpu(args)

@@ -38,10 +38,20 @@ def _shift(a, d, fill):
     return out
 
 
-def classify(fluid, box_shape, offset, inlet_z=None, outlet_z=None, normal_fn=None):
+def classify(fluid, box_shape, offset, inlet_z=None, outlet_z=None, normal_fn=None, openings=None):
     """Node set of a fluid mask given on a sub-box at `offset` of a box of
     `box_shape` (lattice cells). inlet_z / outlet_z: z index of the inlet and
-    outlet planes (box faces); normal_fn(points[k,3]) -> outward normals."""
+    outlet planes (box faces); normal_fn(points[k,3]) -> outward normals.
+    `openings` generalises the planes: a list of (kind, axis, index, normal,
+    select) with kind "inlet" (at most one) or "outlet", the boundary nodes
+    whose coordinate along `axis` equals `index`, optionally restricted by
+    select(coords[k,3]) -> bool[k]; outlets are numbered in list order."""
+    if openings is None:
+        openings = []
+        if inlet_z is not None:
+            openings.append(("inlet", 2, inlet_z, (0.0, 0.0, -1.0), None))
+        if outlet_z is not None:
+            openings.append(("outlet", 2, outlet_z, (0.0, 0.0, 1.0), None))
     F = fluid.astype(bool)
     nf = ~F
     # 26-neighbourhood test against non-fluid; cells outside the sub-box are
@@ -89,10 +99,29 @@ def classify(fluid, box_shape, offset, inlet_z=None, outlet_z=None, normal_fn=No
     kind = np.zeros(F.shape, np.uint8)
     inl = np.zeros_like(F)
     outl = np.zeros_like(F)
-    if inlet_z is not None:
-        inl[:, :, inlet_z - oz] = B[:, :, inlet_z - oz]
-    if outlet_z is not None:
-        outl[:, :, outlet_z - oz] = B[:, :, outlet_z - oz] & ~inl[:, :, outlet_z - oz]
+    inlet_normal = np.zeros(3)
+    out_masks, out_normals = [], []
+    for what, axis, index, normal, select in openings:
+        loc = index - offset[axis]
+        m = np.zeros_like(F)
+        if 0 <= loc < F.shape[axis]:
+            sl = [slice(None)] * 3
+            sl[axis] = loc
+            m[tuple(sl)] = B[tuple(sl)]
+        m &= ~inl & ~outl
+        if select is not None and m.any():
+            pts = np.stack(np.nonzero(m), axis=1) + np.array(offset)
+            keep = np.asarray(select(pts.astype(np.float64)), bool)
+            sub = np.zeros_like(F)
+            sub[tuple((pts - np.array(offset))[keep].T)] = True
+            m = sub
+        if what == "inlet":
+            inl |= m
+            inlet_normal = np.asarray(normal, np.float64)
+        else:
+            outl |= m
+            out_masks.append(m)
+            out_normals.append(np.asarray(normal, np.float64))
     wall = B & ~inl & ~outl
     kind[inl] = 1
     kind[outl] = 2
@@ -114,12 +143,13 @@ def classify(fluid, box_shape, offset, inlet_z=None, outlet_z=None, normal_fn=No
         "coords": coords,
         "kind": kinds,
         "inlet": idx[np.nonzero(inl)],
-        "inlet_normal": np.array([0.0, 0.0, -1.0]),
-        "outlet_0": idx[np.nonzero(outl)],
-        "outlet_normal_0": np.array([0.0, 0.0, 1.0]),
+        "inlet_normal": inlet_normal,
         "wall": idx[np.nonzero(wall)],
         "nearwall": nearwall,
     }
+    for k, (m, nrm) in enumerate(zip(out_masks, out_normals)):
+        topo["outlet_%d" % k] = idx[np.nonzero(m)]
+        topo["outlet_normal_%d" % k] = nrm
     if normal_fn is not None:
         topo["nearwall_normal"] = normal_fn(coords[nearwall].astype(np.float64))
     else:
@@ -265,3 +295,137 @@ def parabolic_inlet(topo, u_max, radius=None, centre=None):
     v = np.zeros((len(xy), 3))
     v[:, 2] = np.maximum(0.0, u_max * (1.0 - r2 / (R * R)))
     return v
+
+
+# ------------------------------------------------------ branching vessels ---
+def _voxelise(field, box, lo, hi):
+    """Fluid mask (field < 0) on the sub-box [lo, hi) of `box`, z-slab by z-slab."""
+    lo = [max(0, int(v)) for v in lo]
+    hi = [min(b, int(v)) for b, v in zip(box, hi)]
+    gx, gy = np.meshgrid(np.arange(lo[0], hi[0], dtype=np.float64), np.arange(lo[1], hi[1], dtype=np.float64),
+                         indexing="ij")
+    fluid = np.zeros((hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]), bool)
+    for z in range(lo[2], hi[2]):
+        p = np.stack([gx.ravel(), gy.ravel(), np.full(gx.size, float(z))], axis=1)
+        fluid[:, :, z - lo[2]] = (field(p) < 0).reshape(gx.shape)
+    return fluid, tuple(lo)
+
+
+def _perpendiculars(d):
+    d = d / np.linalg.norm(d)
+    a = np.array([0.0, 1.0, 0.0]) if abs(d[1]) < 0.9 else np.array([1.0, 0.0, 0.0])
+    n1 = np.cross(d, a)
+    n1 /= np.linalg.norm(n1)
+    return n1, np.cross(d, n1)
+
+
+def _tube(p0, d, length, radius, wiggle=(0.0, 0.0)):
+    """Signed distance of a straight capsule from p0 along d (length, radius)
+    whose axis is displaced by wiggle[0] sin(pi s / L) n1 + wiggle[1]
+    sin(2 pi s / L) n2 (zero at both ends)."""
+    p0 = np.asarray(p0, np.float64)
+    d = np.asarray(d, np.float64) / np.linalg.norm(d)
+    n1, n2 = _perpendiculars(d)
+
+    def f(p):
+        s = np.clip((p - p0) @ d, 0.0, length)
+        c = p0 + s[:, None] * d
+        c = c + (wiggle[0] * np.sin(np.pi * s / length))[:, None] * n1
+        c = c + (wiggle[1] * np.sin(2 * np.pi * s / length))[:, None] * n2
+        return np.linalg.norm(p - c, axis=1) - radius
+    return f
+
+
+def y_bifurcation(seed=2, box=(256, 256, 348), parent=(24.0, 200.0), daughters=((18.0, 180.0), (16.0, 180.0)),
+                  angle_deg=35.0):
+    """Y-bifurcation: a parent tube along +z from the inlet plane z = 0 to the
+    branch point at z = parent length, and two daughters at +-angle in the
+    x-z plane, their centerlines displaced by seeded smooth wiggles (at most
+    2 lu, zero at the ends). The daughters leave through the top face z = Z-1
+    (an oblique cut), split into outlet 0 (x < X/2) and outlet 1."""
+    X, Y, Z = box
+    rng = np.random.default_rng(seed)
+    cx, cy = X / 2 - 0.5 + 0.31, Y / 2 - 0.5 + 0.17
+    rp, lp = parent
+    tubes = [_tube((cx, cy, -30.0), (0, 0, 1), lp + 30.0, rp, rng.uniform(-2, 2, 2))]
+    a = math.radians(angle_deg)
+    for sign, (rd, ld) in zip((-1.0, 1.0), daughters):
+        d = np.array([sign * math.sin(a), 0.0, math.cos(a)])
+        # continue past the top face so that the face cuts the tube open
+        over = (Z + 30 - lp) / math.cos(a)
+        tubes.append(_tube((cx, cy, lp), d, max(ld, over), rd, rng.uniform(-2, 2, 2)))
+
+    def field(p):
+        return np.minimum.reduce([t(p) for t in tubes])
+
+    fluid, off = _voxelise(field, box, (0, cy - 40, 0), (X, cy + 40, Z))
+    openings = [("inlet", 2, 0, (0.0, 0.0, -1.0), None),
+                ("outlet", 2, Z - 1, (0.0, 0.0, 1.0), lambda c: c[:, 0] < X / 2),
+                ("outlet", 2, Z - 1, (0.0, 0.0, 1.0), None)]
+    topo = classify(fluid, box, off, normal_fn=lambda pts: _normals_from_field(field, pts), openings=openings)
+    topo["axis_centre"] = np.array([cx, cy])
+    topo["radius"] = np.array([rp])
+    return topo
+
+
+def saccular_aneurysm(box=(1024, 512, 512), radius=20.0, bend_radius=120.0, sac_radius=40.0, neck=15.0,
+                      x0=100.0, z0=100.0):
+    """90-degree curved tube with a spherical sac on the outer wall of the bend.
+    The tube rises along +z from the inlet plane z = 0 to z0 at x = x0, bends
+    through a quarter circle of bend_radius in the x-z plane, and runs along
+    +x to the outlet plane x = X-1. The sac's centre lies on the bend's
+    45-degree ray, sac_radius - neck beyond the outer wall, so the sphere
+    overlaps the tube wall by `neck` lu. Also returns the sac centre under
+    "sac_centre"."""
+    X, Y, Z = box
+    yc = Y / 2 - 0.5 + 0.23
+    cb = np.array([x0 + bend_radius, yc, z0])  # bend centre
+    t_in = _tube((x0, yc, -30.0), (0, 0, 1), z0 + 30.0, radius)
+    t_out = _tube((x0 + bend_radius, yc, z0 + bend_radius), (1, 0, 0), X + 30.0 - x0 - bend_radius, radius)
+    ray = np.array([-math.cos(math.pi / 4), 0.0, math.sin(math.pi / 4)])
+    sac = cb + (bend_radius + radius + sac_radius - neck) * ray
+
+    def bend(p):
+        v = p - cb
+        phi = np.arctan2(v[:, 2], -v[:, 0])  # 0 at the tube's start, pi/2 at its end
+        rho = np.hypot(v[:, 0], v[:, 2])
+        d = np.hypot(rho - bend_radius, v[:, 1]) - radius
+        return np.where((phi >= 0) & (phi <= math.pi / 2), d, np.inf)
+
+    def field(p):
+        return np.minimum.reduce([t_in(p), t_out(p), bend(p), np.linalg.norm(p - sac, axis=1) - sac_radius])
+
+    lo = (x0 - radius - 3, yc - max(radius, sac_radius) - 3, 0)
+    hi = (X, yc + max(radius, sac_radius) + 4, max(z0 + bend_radius + radius, sac[2] + sac_radius) + 4)
+    fluid, off = _voxelise(field, box, lo, hi)
+    openings = [("inlet", 2, 0, (0.0, 0.0, -1.0), None), ("outlet", 0, X - 1, (1.0, 0.0, 0.0), None)]
+    topo = classify(fluid, box, off, normal_fn=lambda pts: _normals_from_field(field, pts), openings=openings)
+    topo["sac_centre"] = sac
+    topo["sac_radius"] = np.array([sac_radius])
+    topo["axis_centre"] = np.array([x0, yc])
+    topo["radius"] = np.array([radius])
+    return topo
+
+
+def sac_wall_targets(topo, margin=3.0):
+    """Near-wall list entries on the sac: within sac_radius + margin of the sac
+    centre and farther than sac_radius - 2 margin from it (its wall layer)."""
+    nw = np.asarray(topo["nearwall"], np.int64)
+    c = topo["coords"][nw].astype(np.float64)
+    r = np.linalg.norm(c - topo["sac_centre"], axis=1)
+    R = float(topo["sac_radius"][0])
+    return np.nonzero((r <= R + margin) & (r >= R - 2 * margin))[0].astype(np.int64)
+
+
+def inlet_disc_profile(topo, mean, radius=None):
+    """Parabolic inflow with the given mean velocity on the inlet disc, along
+    -inlet_normal, centred on the inlet nodes ([n_inlet, 3])."""
+    xyz = topo["coords"][topo["inlet"]].astype(np.float64)
+    nrm = np.asarray(topo["inlet_normal"], np.float64)
+    c = xyz.mean(axis=0)
+    rel = xyz - c
+    rel -= np.outer(rel @ nrm, nrm)
+    r2 = (rel ** 2).sum(axis=1)
+    R = float(topo["radius"][0]) if radius is None else radius
+    v = np.maximum(0.0, 2.0 * mean * (1.0 - r2 / (R * R)))
+    return v[:, None] * (-nrm)[None, :]

@@ -219,13 +219,21 @@ int lbm_get_info(lbm_engine* e, int64_t* n_nodes, int64_t* ld, int64_t* n_segmen
  * halfway bounce-back walls, the anti-bounce-back outlet at the engine's
  * outlet density, and an inlet whose speed along -inlet_normal at inlet node
  * i is v_i = sum_j coeffs[j] basis[j][i] (the engine's own inlet profile is
- * not used), times the engine's waveform factor of each step. Objective:
- *   J = (1/T) sum_{t=1..T} sum_{k in target} |tau_k^t|^2,
+ * not used), times the engine's waveform factor of each step. Objective
+ * (desc->objective):
+ *   LBM_ADJOINT_WSS2: J = (1/T) sum_{t=1..T} sum_{k in target} |tau_k^t|^2,
+ *   LBM_ADJOINT_OSI:  J = mean over the targets of their OSI over the T steps,
  * tau_k^t the wall-shear traction vector of near-wall entry k at step t, with
  * the definition and scale of lbm_get_wss. With gradient = 1 it also returns
  * dJ/dcoeffs, dJ/dtau and dJ/dv_i from a hand-written discrete adjoint: the
  * state is checkpointed every checkpoint_every steps, and the reverse sweep
  * recomputes each segment from its checkpoint (memory ~ (T/K + K) states). */
+/* Objectives of lbm_adjoint_run. LBM_ADJOINT_OSI is the mean over the
+ * targets of OSI_k = (1 - |A_k| / M_k) / 2 with A_k = sum_t tau_k^t and
+ * M_k = sum_t |tau_k^t| (the accumulators of lbm_get_wss, taken over the
+ * run's T steps; a target whose M_k is 0 contributes 0). */
+typedef enum { LBM_ADJOINT_WSS2 = 0, LBM_ADJOINT_OSI = 1 } lbm_adjoint_objective;
+
 typedef struct {
     int64_t n_steps;            /* T >= 1 */
     int64_t checkpoint_every;   /* K >= 1; ignored without gradient */
@@ -235,6 +243,7 @@ typedef struct {
     int32_t n_coeffs;
     const double* basis;        /* [n_coeffs][n_inlet], caller's inlet order */
     const double* coeffs;       /* [n_coeffs] */
+    int32_t objective;          /* lbm_adjoint_objective */
 } lbm_adjoint_desc;
 
 typedef struct {

@@ -13,8 +13,13 @@
 //   with eq_q(u) = 1 + 4.5 (c_q.u)^2 - 1.5 u^2, u the velocity of f^t at n,
 //   v(n) the inlet speed (along -n_in) and s_t the waveform factor of step t.
 // This is the engine's physics step (same links, same corrections) written as
-// a push. Objective, over the target near-wall nodes k:
+// a push. Objective, over the target near-wall nodes k, either the
+// time-averaged squared wall shear
 //   J = (1/T) sum_{t=1..T} sum_k |tau_k^t|^2,
+// or the mean oscillatory shear index
+//   J = (1/n) sum_k (1 - |A_k| / M_k) / 2,  A_k = sum_t tau_k^t, M_k = sum_t |tau_k^t|
+// (dJ/dtau_k^t = dJ/dA_k + dJ/dM_k tau_k^t / |tau_k^t|, with the sums taken
+// from the forward sweep), where
 //   tau^t = C_w sum_q (f^t_q - feq_q(f^{t-1})) M_q,  M_q = (c_q.n)(c_q - (c_q.n) n)
 // which is the engine's wall shear stress of step t (its f_eq comes from the
 // previous state's moments).
@@ -242,7 +247,22 @@ struct ObjArgs {
     double* mom;             // [T + 1][n_target][4]: drho, u of f^t
     double cw, inv_T;
     double* J;
+    int osi;                 // objective: 0 time-averaged WSS^2, 1 mean OSI
+    double* acc;             // OSI: [n_target][4] sum of tau (3) and of |tau|
+    const double* coef;      // OSI: [n_target][4] dJ/dtau^t = coef[0..2] + coef[3] tau^t / |tau^t|
 };
+
+// dJ/dtau^t of one target for the objective
+__device__ __forceinline__ void objective_dtau(int osi, const double* coef, double inv_T, const double tau[3],
+                                               double out[3]) {
+    if (!osi) {
+        for (int c = 0; c < 3; ++c) out[c] = 2.0 * inv_T * tau[c];
+        return;
+    }
+    const double m = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
+    const double k = m > 0.0 ? coef[3] / m : 0.0;
+    for (int c = 0; c < 3; ++c) out[c] = coef[c] + k * tau[c];
+}
 
 // Objective term of step t at the target nodes (forward sweep), one warp per
 // target and one lane per direction: records the moments of f^t and adds
@@ -274,7 +294,17 @@ __global__ void adj_objective_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, i
             const double t0 = a.cw * warp_sum(f * (c0 - cn * nrm[0]));
             const double t1 = a.cw * warp_sum(f * (c1 - cn * nrm[1]));
             const double t2 = a.cw * warp_sum(f * (c2 - cn * nrm[2]));
-            if (lane == 0) jl = a.inv_T * (t0 * t0 + t1 * t1 + t2 * t2);
+            if (lane == 0) {
+                if (a.osi) {
+                    double* ac = a.acc + 4 * (long long)k;
+                    ac[0] += t0;
+                    ac[1] += t1;
+                    ac[2] += t2;
+                    ac[3] += sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+                } else {
+                    jl = a.inv_T * (t0 * t0 + t1 * t1 + t2 * t2);
+                }
+            }
         }
         if (lane == 0) {
             mt[0] = drho;
@@ -389,23 +419,27 @@ __global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restric
     const double* nrm = a.nw_normal + 3 * (long long)a.nw[k];
     const double cn = c0 * nrm[0] + c1 * nrm[1] + c2 * nrm[2];
     const double m0 = c0 - cn * nrm[0], m1 = c1 - cn * nrm[1], m2 = c2 - cn * nrm[2];
-    const double scale = 2.0 * a.inv_T * a.cw;
+    const double* coef = a.osi ? a.coef + 4 * (long long)k : nullptr;
     double g = 0.0;
     if (t >= 1) {
         const double* mp = a.mom + ((long long)(t - 1) * a.n_target + k) * 4;
         const R up[3] = {(R)mp[1], (R)mp[2], (R)mp[3]};
         const double fne = on ? (double)(D[(long long)q * a.ld + n] - deq<R, Q>(q, (R)mp[0], up)) : 0.0;
         const double f = fne * cn;
-        const double t0 = a.cw * warp_sum(f * m0), t1 = a.cw * warp_sum(f * m1), t2 = a.cw * warp_sum(f * m2);
-        g = scale * cn * (t0 * m0 + t1 * m1 + t2 * m2);
+        const double tau[3] = {a.cw * warp_sum(f * m0), a.cw * warp_sum(f * m1), a.cw * warp_sum(f * m2)};
+        double dt[3];
+        objective_dtau(a.osi, coef, a.inv_T, tau, dt);
+        g = a.cw * cn * (dt[0] * m0 + dt[1] * m1 + dt[2] * m2);
     }
     if (t < T) {
         const double* mt = a.mom + ((long long)t * a.n_target + k) * 4;
         const R ut[3] = {(R)mt[1], (R)mt[2], (R)mt[3]};
         const double fne = on ? (double)(Dn[(long long)q * a.ld + n] - deq<R, Q>(q, (R)mt[0], ut)) : 0.0;
         const double f = fne * cn;
-        const double t0 = a.cw * warp_sum(f * m0), t1 = a.cw * warp_sum(f * m1), t2 = a.cw * warp_sum(f * m2);
-        const double gq = on ? scale * cn * (t0 * m0 + t1 * m1 + t2 * m2) : 0.0;
+        const double tau[3] = {a.cw * warp_sum(f * m0), a.cw * warp_sum(f * m1), a.cw * warp_sum(f * m2)};
+        double dt[3];
+        objective_dtau(a.osi, coef, a.inv_T, tau, dt);
+        const double gq = on ? a.cw * cn * (dt[0] * m0 + dt[1] * m1 + dt[2] * m2) : 0.0;
         // sum_r gq_r d feq_r / d f_q = A + B . c_q at the moments of f^t
         const double u[3] = {mt[1], mt[2], mt[3]};
         const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
@@ -777,6 +811,8 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         lam[1] = ar.get<R>(field);
     }
     double* mom = ar.get<double>((size_t)(T + 1) * std::max(nt, 1) * 4);
+    double* osi_acc = ar.get<double>((size_t)std::max(nt, 1) * 4);
+    double* osi_coef = ar.get<double>((size_t)std::max(nt, 1) * 4);
     double* speed = ar.get<double>(std::max(s.n_in, 1));
     double* dspeed = ar.get<double>(std::max(s.n_in, 1));
     double* scal = ar.get<double>(2 * N_PARTIALS);  // J, then dJ/domega partial sums
@@ -801,6 +837,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         if (s.n_in) cudaMemcpyAsync(speed, s.speed.data(), sizeof(double) * s.n_in, cudaMemcpyHostToDevice, st);
         cudaMemsetAsync(dspeed, 0, sizeof(double) * std::max(s.n_in, 1), st);
         cudaMemsetAsync(scal, 0, 2 * N_PARTIALS * sizeof(double), st);
+        cudaMemsetAsync(osi_acc, 0, sizeof(double) * 4 * std::max(nt, 1), st);
         // the host vectors above die at the end of this block
         cudaError_t ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) {
@@ -830,6 +867,9 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     oa.cw = s.wss_c;
     oa.inv_T = 1.0 / (double)T;
     oa.J = scal;
+    oa.osi = s.objective == 1;
+    oa.acc = osi_acc;
+    oa.coef = osi_coef;
 
     const dim3 grid((unsigned)((s.n + AT - 1) / AT));
     const unsigned tgrid = (unsigned)((nt + 3) / 4);  // one warp per target, 4 per block
@@ -887,6 +927,34 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         fT = seg[T - tl];
     }
     if (s.final_pop) adj_store_kernel<R, Q><<<grid, AT, 0, st>>>(fT, s.ld, s.n, s.final_pop);
+    // mean OSI: J and its derivative w.r.t. each target's sums A = sum tau,
+    // M = sum |tau| (OSI = (1 - |A| / M) / 2), once the forward sweep is done
+    double J_osi = 0.0;
+    if (oa.osi && nt) {
+        std::vector<double> acc(4 * (size_t)nt), coef(4 * (size_t)nt, 0.0);
+        cudaMemcpyAsync(acc.data(), osi_acc, sizeof(double) * acc.size(), cudaMemcpyDeviceToHost, st);
+        cudaError_t e1 = cudaStreamSynchronize(st);
+        if (e1 != cudaSuccess) {
+            o.err = std::string("adjoint OSI sums: ") + cudaGetErrorString(e1);
+            return -2;
+        }
+        for (int k = 0; k < nt; ++k) {
+            const double* a4 = &acc[4 * (size_t)k];
+            const double A = std::sqrt(a4[0] * a4[0] + a4[1] * a4[1] + a4[2] * a4[2]), M = a4[3];
+            if (!(M > 0.0)) continue;
+            J_osi += 0.5 * (1.0 - A / M) / nt;
+            if (A > 0.0)
+                for (int c = 0; c < 3; ++c) coef[4 * (size_t)k + c] = -0.5 * a4[c] / (A * M * nt);
+            coef[4 * (size_t)k + 3] = 0.5 * A / (M * M * nt);
+        }
+        cudaMemcpyAsync(osi_coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice, st);
+        // coef must stay alive until the copy has run
+        e1 = cudaStreamSynchronize(st);
+        if (e1 != cudaSuccess) {
+            o.err = std::string("adjoint OSI coefficients: ") + cudaGetErrorString(e1);
+            return -2;
+        }
+    }
     cudaEventRecord(ev.e[1], st);
     cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) {
@@ -941,6 +1009,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         o.J += hs[i];
         o.dJ_domega += hs[N_PARTIALS + i];
     }
+    if (oa.osi) o.J = J_osi;
     o.dJ_dspeed.assign(s.n_in, 0.0);
     if (s.gradient && s.n_in)
         cudaMemcpy(o.dJ_dspeed.data(), dspeed, sizeof(double) * s.n_in, cudaMemcpyDeviceToHost);

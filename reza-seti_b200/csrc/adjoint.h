@@ -16,6 +16,7 @@ struct AdjointSetup {
     int Q = 19;
     bool fp64 = false;          // FP64 or FP32 arithmetic and storage
     bool gradient = true;       // false: objective only (forward sweep)
+    int objective = 0;          // 0: time-averaged sum of |WSS|^2, 1: mean OSI over the targets
     int n = 0;
     long long ld = 0;
     const void* meta = nullptr;      // Meta<Q>::T [n]

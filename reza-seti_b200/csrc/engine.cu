@@ -988,9 +988,12 @@ int lbm_adjoint_run(lbm_engine* e, const lbm_adjoint_desc* d, int32_t gradient, 
     const int n_in = e->nin();
     if (d->n_coeffs < 0 || (d->n_coeffs > 0 && (!d->coeffs || (n_in > 0 && !d->basis))))
         return e->fail(LBM_ERR_ARGUMENT, "bad inlet coefficients or basis");
+    if (d->objective != LBM_ADJOINT_WSS2 && d->objective != LBM_ADJOINT_OSI)
+        return e->fail(LBM_ERR_ARGUMENT, "unknown adjoint objective");
     if (e->pop_step != e->step) return e->fail(LBM_ERR_STATE, "populations of the last step were not observed");
     cudaSetDevice(e->device);
     AdjointSetup s;
+    s.objective = d->objective;
     s.Q = e->Q;
     s.fp64 = d->precision == LBM_STORE_F64;
     s.gradient = gradient != 0;

@@ -24,6 +24,7 @@ STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 BC_REFERENCE, BC_PHYSICS = 0, 1
 FLOW_CONSTANT, FLOW_PULSATILE, FLOW_HARMONIC = 0, 1, 2
 FLAG_ZERO_SKIP, FLAG_NONFINITE = 1, 2
+ADJOINT_OBJECTIVE = {"wss2": 0, "osi": 1}
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -48,7 +49,7 @@ class LbmAdjointDesc(ctypes.Structure):
     _fields_ = [
         ("n_steps", ctypes.c_int64), ("checkpoint_every", ctypes.c_int64), ("precision", ctypes.c_int32),
         ("n_target", ctypes.c_int32), ("target", _i64p), ("n_coeffs", ctypes.c_int32),
-        ("basis", _f64p), ("coeffs", _f64p),
+        ("basis", _f64p), ("coeffs", _f64p), ("objective", ctypes.c_int32),
     ]
 
 

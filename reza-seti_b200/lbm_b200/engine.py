@@ -180,9 +180,10 @@ class Engine:
         return v.value
 
     def adjoint(self, n_steps, targets, basis, coeffs, *, gradient=True, checkpoint_every=100,
-                precision="f32", final_populations=False):
-        """Time-averaged WSS^2 objective over the near-wall entries `targets`
-        and, with `gradient`, its adjoint gradient (lbm_adjoint_run). The
+                precision="f32", final_populations=False, objective="wss2"):
+        """Objective over the near-wall entries `targets` — "wss2", the
+        time-averaged sum of |WSS|^2, or "osi", their mean oscillatory shear
+        index — and, with `gradient`, its adjoint gradient (lbm_adjoint_run). The
         inlet speed along -inlet_normal is coeffs @ basis ([n_coeffs, n_inlet]).
         Returns a dict: J, dJ_dtau, grad_coeffs, grad_inlet, forward_ms,
         reverse_ms, steps_recomputed, device_bytes (and populations)."""
@@ -196,6 +197,7 @@ class Engine:
         d.precision = capi.STORAGE[precision]
         d.n_target, d.target = len(targets), _p(targets, capi._i64p)
         d.n_coeffs, d.basis, d.coeffs = len(coeffs), _p(basis, capi._f64p), _p(coeffs, capi._f64p)
+        d.objective = capi.ADJOINT_OBJECTIVE[objective]
         gc = np.zeros(max(1, len(coeffs)))
         gi = np.zeros(max(1, self.n_inlet))
         r = capi.LbmAdjointResult()

@@ -166,3 +166,41 @@ def test_argument_and_state_errors():
     with pytest.raises(capi.LbmError) as ex:
         e.adjoint(10, [0], basis, a)
     assert ex.value.code == capi.LBM_ERR_STATE
+
+
+def test_osi_objective_matches_central_differences():
+    """Mean OSI over the throat under an oscillating inflow that reverses
+    (waveform factor 1 + 1.5 cos(2 pi t / 60)): the FP64 adjoint gradient
+    equals central differences (h = 1e-4) for every coefficient and for tau,
+    and the FP32 adjoint tracks it."""
+    topo = stenosed_pipe()
+    basis = G.zernike_inlet_basis(topo, 8)
+    a = coefficients()
+    targets = G.stenotic_throat_targets(topo, 4.0)
+    T, tau = 180, 0.6
+
+    def make(t):
+        e = Engine(topo, tau=t, storage="f64", bc="physics")
+        e.set_waveform(60.0, [1.5], [0.0])
+        e.set_flow(False, 0.0, harmonic=True)
+        return e
+
+    e = make(tau)
+    r = e.adjoint(T, targets, basis, a, checkpoint_every=40, precision="f64", objective="osi")
+    assert 0.05 < r["J"] < 0.5
+    g_fd = np.zeros(len(a))
+    for j in range(len(a)):
+        ap, am = a.copy(), a.copy()
+        ap[j] += H
+        am[j] -= H
+        g_fd[j] = (e.adjoint(T, targets, basis, ap, gradient=False, precision="f64", objective="osi")["J"] -
+                   e.adjoint(T, targets, basis, am, gradient=False, precision="f64", objective="osi")["J"]) / (2 * H)
+    jt = [make(t).adjoint(T, targets, basis, a, gradient=False, precision="f64", objective="osi")["J"]
+          for t in (tau + H, tau - H)]
+    gt_fd = (jt[0] - jt[1]) / (2 * H)
+    print("osi J", r["J"], "grad", r["grad_coeffs"], g_fd, "tau", r["dJ_dtau"], gt_fd)
+    assert rel(r["grad_coeffs"], g_fd) < 1e-4
+    assert abs(r["dJ_dtau"] - gt_fd) < 1e-4 * abs(gt_fd)
+    r32 = e.adjoint(T, targets, basis, a, checkpoint_every=40, precision="f32", objective="osi")
+    assert abs(r32["J"] - r["J"]) < 1e-4 * r["J"]
+    assert rel(r32["grad_coeffs"], r["grad_coeffs"]) < 1e-2

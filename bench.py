@@ -166,7 +166,10 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """World size, rank, local rank and torch.distributed (or None for one
+    process) from the torchrun environment. Ranks are independent replicas:
+    the process group carries only the barriers and the max-over-ranks time."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -175,12 +178,29 @@ def dist_setup(n_gpus):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
 
-def time_engine(topo, storage, steps, warmup, device, torch, vel, bc="physics", radius=None):
+def max_over_ranks(value, dist, device):
+    """The largest of every rank's value: the job takes as long as its
+    slowest replica."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_mlups(n_nodes, steps, max_ms, world):
+    """Whole-job MLUPS of `world` replicas of n_nodes each over `steps` steps
+    that took at most max_ms."""
+    return n_nodes * steps / (max_ms / 1e3) / 1e6 * world
+
+
+def time_engine(topo, storage, steps, warmup, device, torch, vel, bc="physics", radius=None, before=None):
     from lbm_b200 import Engine
     eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device, bc=bc)
     eng.set_flow(False, vel)
@@ -193,6 +213,8 @@ def time_engine(topo, storage, steps, warmup, device, torch, vel, bc="physics", 
     eng.set_stream(stream.cuda_stream)
     eng.step(warmup)
     torch.cuda.synchronize(device)
+    if before is not None:
+        before()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
@@ -215,23 +237,22 @@ def run_gpu(args):
     S = BYTES_PER_POP[storage]
     Q = 19
 
-    # headline: K steps on the engine stream, CUDA events, barrier + sync both sides
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(device)
+    # headline: K steps on the engine stream, CUDA events, barrier + sync on
+    # both sides of the timed region
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
     with ClockSampler(device) as clk:
         eng, total_ms, ms_step, ms_bnd = time_engine(topo, storage, args.steps, args.warmup, device, torch, vel,
-                                                     args.bc, radius)
-    torch.cuda.synchronize(device)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
+                                                     args.bc, radius, before=barrier)
+    barrier()
+    total_ms = max_over_ranks(total_ms, dist, "cuda")
     clocks = clk.summary()
     info = eng.info()
     flags = eng.flags()
-    mlups = n * args.steps / (total_ms / 1e3) / 1e6 * world
+    mlups = replica_mlups(n, args.steps, total_ms, world)
     ms_per_step = total_ms / args.steps
 
     # roofline of the dominant kernel (stream+collide): algorithmic bytes 2 Q S per node

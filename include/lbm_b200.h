@@ -199,9 +199,11 @@ int lbm_flux_noalloc(const double* f, int64_t n_nodes, int32_t q, const int64_t*
  * zero (the reference would not have streamed it), 2 = non-finite density. */
 int lbm_get_flags(lbm_engine* e, uint32_t* flags);
 
-/* Device time of the last n_steps steps run through lbm_step_timed, per kernel
- * class: the stream+collide kernel and the boundary pre-pass (milliseconds,
- * summed over the steps, CUDA events on the engine's stream). */
+/* Runs n_steps steps like lbm_step and returns their device time per kernel
+ * class (milliseconds, summed over the steps, CUDA events on the engine's
+ * stream): the stream+collide kernel, and the boundary work around it — the
+ * pre-pass (wall shear stress, outlet copy sources) in reference mode, the
+ * post-pass (wall shear stress, open-boundary corrections) in physics mode. */
 int lbm_step_timed(lbm_engine* e, int64_t n_steps, double* step_kernel_ms, double* boundary_kernel_ms);
 
 /* Sizes: nodes, padded leading dimension, segments, near-wall nodes, outlet

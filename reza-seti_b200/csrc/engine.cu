@@ -512,6 +512,68 @@ int init_from_obs(lbm_engine* e) {
     return 0;
 }
 
+// Physics mode: per step the stream+collide kernel, then one post-pass with
+// that step's wall shear stress and the open-boundary corrections of its
+// store (which streams into the next step). No pre-pass: physics mode has no
+// outlet copy sources. Timed runs record ev[2i] before step kernel i and
+// ev[2i+1] before its post-pass; ev[2n] after the last post-pass. A WSS
+// hand-off left pending by an earlier reference-style sequence is reduced
+// first (never the case in physics mode, where every post-pass reduces it).
+int run_steps_physics(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
+    const bool timed = t_step || t_bnd;
+    const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
+    for (int64_t i = 0; i < n_steps; ++i) {
+        const int64_t t = e->step + 1;
+        int obs = 0;
+        if (e->observe && i >= n_steps - 2) obs |= 2;
+        if (e->observe && i == n_steps - 1) obs |= 1;
+        double* mom = e->obs_mom[t % 2];
+        const int phase = e->phase;
+        const double scale = inlet_factor(e, e->step + 1, pulsatile ? e->runtime + e->dt : e->runtime);
+        int rc = dispatch(e, [&](auto tag) {
+            using S = typename decltype(tag)::St;
+            constexpr int Q = decltype(tag)::q;
+            cudaError_t ce = cudaSuccess;
+            if (e->wss_pending) {
+                ce = launch_boundary<S, Q>(boundary_args<S, Q>(e, 0.0, true, false), phase, e->stream);
+                if (ce != cudaSuccess) return e->cuda_fail(ce, "wall shear kernel");
+                e->wss_pending = false;
+            }
+            if (timed) cudaEventRecord(e->evpool[2 * i], e->stream);
+            ce = launch_step<S, Q>(step_args<S, Q>(e, 0.0, mom), phase, e->bc, obs, e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "step kernel");
+            if (timed) cudaEventRecord(e->evpool[2 * i + 1], e->stream);
+            ce = launch_post<S, Q>(boundary_args<S, Q>(e, 0.0, e->nw() > 0, false), open_args<S, Q>(e, scale),
+                                   e->stream);
+            return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "post-step kernel");
+        });
+        if (rc) return rc;
+        if (obs & 2) e->mom_step[t % 2] = t;
+        if (obs & 1) e->pop_step = t;
+        e->phase ^= 1;
+        e->step = t;
+        if (pulsatile) e->runtime += e->dt;
+        e->fresh = false;
+    }
+    if (timed) {
+        cudaEventRecord(e->evpool[2 * n_steps], e->stream);
+        cudaEventRecord(e->evpool[2 * n_steps + 1], e->stream);
+        cudaError_t ce = cudaEventSynchronize(e->evpool[2 * n_steps + 1]);
+        if (ce != cudaSuccess) return e->cuda_fail(ce, "timed steps");
+        double ms_step = 0, ms_bnd = 0;
+        for (int64_t i = 0; i < n_steps; ++i) {
+            float a = 0, b = 0;
+            cudaEventElapsedTime(&a, e->evpool[2 * i], e->evpool[2 * i + 1]);
+            cudaEventElapsedTime(&b, e->evpool[2 * i + 1], e->evpool[2 * i + 2]);
+            ms_step += a;
+            ms_bnd += b;
+        }
+        if (t_step) *t_step = ms_step;
+        if (t_bnd) *t_bnd = ms_bnd;
+    }
+    return 0;
+}
+
 int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
     if (n_steps < 0) return e->fail(LBM_ERR_ARGUMENT, "negative step count");
     if (n_steps == 0) return 0;
@@ -531,6 +593,7 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
             e->evpool.push_back(ev);
         }
     }
+    if (e->bc == LBM_BC_PHYSICS) return run_steps_physics(e, n_steps, t_step, t_bnd);
     for (int64_t i = 0; i < n_steps; ++i) {
         const int64_t t = e->step + 1;
         const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;

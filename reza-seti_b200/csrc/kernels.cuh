@@ -656,11 +656,9 @@ struct OpenArgs {
 };
 
 template <class S, int Q>
-__global__ void open_boundary_kernel(OpenArgs<S, Q> a) {
+__device__ __forceinline__ void open_item(const OpenArgs<S, Q>& a, int i) {
     using L = Lat<Q>;
     using C = typename Store<S>::C;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n_in + a.n_out) return;
     const bool inlet = i < a.n_in;
     const int k = inlet ? i : i - a.n_in;
     const int n = inlet ? a.in_node[k] : a.out_node[k];
@@ -696,6 +694,13 @@ __global__ void open_boundary_kernel(OpenArgs<S, Q> a) {
         Store<S>::put(slot, (C)v);
     }
 }
+
+template <class S, int Q>
+__global__ void open_boundary_kernel(OpenArgs<S, Q> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.n_in + a.n_out) open_item<S, Q>(a, i);
+}
+
 
 // Boundary pass, launched before the step kernel of each step:
 //  * items [0, n_wss): wall shear stress of the previous step's near-wall
@@ -739,6 +744,22 @@ __global__ void boundary_kernel(BoundaryArgs<S, Q> a) {
         if ((m >> oq) & 1) idx = (long long)oq * a.ld + (src + seg_row<Q>(a.seg_base, a.seg_delta, src, m)[oq]);
     }
     a.out_buf[(long long)k * Q + q] = Store<S>::get(a.pop + idx);
+}
+
+// Physics-mode pass after each step kernel: the wall shear stress of the
+// step just taken (items [0, n_wss)) and the open-boundary corrections of its
+// store (then one item per inlet / outlet node). The two touch disjoint data
+// (the near-wall hand-off buffers and accumulators; the inlet and outlet
+// nodes' bounce-back slots), so one launch does both.
+template <class S, int Q>
+__global__ void post_kernel(BoundaryArgs<S, Q> b, OpenArgs<S, Q> o) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < b.n_wss) {
+        wall_shear<S, Q>(b, (int)i);
+        return;
+    }
+    const long long j = i - b.n_wss;
+    if (j < (long long)o.n_in + o.n_out) open_item<S, Q>(o, (int)j);
 }
 
 }  // namespace lbm

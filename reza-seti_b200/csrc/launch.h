@@ -20,6 +20,11 @@ cudaError_t launch_boundary(const BoundaryArgs<S, Q>& a, int phase, cudaStream_t
 template <class S, int Q>
 cudaError_t launch_open(const OpenArgs<S, Q>& a, cudaStream_t st);
 
+// Physics mode: wall shear stress of the step just taken and the
+// open-boundary corrections of its store, in one launch.
+template <class S, int Q>
+cudaError_t launch_post(const BoundaryArgs<S, Q>& b, const OpenArgs<S, Q>& o, cudaStream_t st);
+
 // Fills natural-layout populations with the lattice weights (f = w).
 cudaError_t launch_fill_weights(double* obs_pop, long long ld, int n, int q, cudaStream_t st);
 

@@ -116,10 +116,20 @@ cudaError_t launch_open(const OpenArgs<S, Q>& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class S, int Q>
+cudaError_t launch_post(const BoundaryArgs<S, Q>& b, const OpenArgs<S, Q>& o, cudaStream_t st) {
+    const long long items = (long long)b.n_wss + o.n_in + o.n_out;
+    if (items == 0) return cudaSuccess;
+    const int tpb = 128;
+    post_kernel<S, Q><<<(unsigned)((items + tpb - 1) / tpb), tpb, 0, st>>>(b, o);
+    return cudaGetLastError();
+}
+
 #define LBM_INSTANTIATE(S, Q)                                                                          \
     template cudaError_t launch_step<S, Q>(const StepArgs<S, Q>&, int, int, int, cudaStream_t);        \
     template cudaError_t launch_init<S, Q>(const StepArgs<S, Q>&, int, cudaStream_t);                  \
     template cudaError_t launch_boundary<S, Q>(const BoundaryArgs<S, Q>&, int, cudaStream_t);          \
-    template cudaError_t launch_open<S, Q>(const OpenArgs<S, Q>&, cudaStream_t);
+    template cudaError_t launch_open<S, Q>(const OpenArgs<S, Q>&, cudaStream_t);                      \
+    template cudaError_t launch_post<S, Q>(const BoundaryArgs<S, Q>&, const OpenArgs<S, Q>&, cudaStream_t);
 
 }  // namespace lbm

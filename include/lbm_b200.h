@@ -262,6 +262,55 @@ typedef struct {
 
 int lbm_adjoint_run(lbm_engine* e, const lbm_adjoint_desc* desc, int32_t gradient, lbm_adjoint_result* result);
 
+/* ---------------------------------------------------- geometry pipeline ---
+ * Builds the node set of an lbm_desc from STL triangles on the GPU, with the
+ * results of the reference's setup chain: Reader::readSTLASCII
+ * (GeometryReader.cpp:74-158), Geometry (ComplexGeometry.cpp:83-662: bounding
+ * box, grid at spacing 2 x grid_size, +z ray-parity labelling, boundary
+ * points, inlet / outlet planes, wall points) and SubDomain::CreateNodes,
+ * IdentifyNextToWallLattices, calculateBoundaryNormals (Subdomain.cpp:364-572).
+ * Node coordinates are grid indices; nodes are in the reference's
+ * Involved_Lat_ order (x-major, z-fastest). Errors: lbm_last_error(NULL). */
+
+/* An inlet or outlet plane of the reference's config.txt (LBM.h:129-168):
+ * boundary points within 2.5e-2 of `coordinate` on `axis` and inside the
+ * ranges of the other two axes (+-infinity when the config gives none). */
+typedef struct {
+    int32_t outlet;            /* 0: inlet, 1: outlet */
+    int32_t axis;              /* plane: 0 x, 1 y, 2 z */
+    double coordinate;
+    double normal[3];
+    double range[3][2];        /* [axis][lo, hi] */
+} lbm_opening;
+
+typedef struct {
+    int64_t n_triangles;
+    const double* triangles;   /* [n_triangles][12]: vertex 1, 2, 3 (x, y, z), then the file's facet normal */
+    double grid_size;          /* config grid_size (SimulationParameters::dx); grid spacing = 2 x grid_size */
+    int32_t n_openings;
+    const lbm_opening* openings; /* inlets and outlets in config order; outlets are numbered in this order */
+    int32_t device;
+} lbm_voxel_desc;
+
+typedef struct lbm_voxel lbm_voxel;
+
+/* Reads an ASCII STL with the line grammar of Reader::readSTLASCII into a
+ * malloc'd [n][12] array (layout of lbm_voxel_desc.triangles); release it
+ * with lbm_free. */
+int lbm_stl_read_ascii(const char* path, int64_t* n_triangles, double** triangles);
+void lbm_free(void* p);
+
+int lbm_voxelise(const lbm_voxel_desc* desc, lbm_voxel** out);
+/* Grid points per axis, grid origin (bounding-box minimum), spacing, node and
+ * near-wall counts, wall-clock build time (ms). Any may be NULL. */
+int lbm_voxel_info(const lbm_voxel* v, int32_t dims[3], double origin[3], double* spacing, int64_t* n_nodes,
+                   int64_t* n_nearwall, double* build_ms);
+/* Points the node and boundary fields of desc (n_nodes ... nearwall_normals,
+ * and spacing) at v's arrays, valid until lbm_voxel_destroy; the caller sets
+ * lattice, storage, bc_mode, device, tau and dt. */
+int lbm_voxel_describe(const lbm_voxel* v, lbm_desc* desc);
+int lbm_voxel_destroy(lbm_voxel* v);
+
 /* Message of the last failed call on e (or of the last failed lbm_create when
  * e is NULL). Never NULL. */
 const char* lbm_last_error(const lbm_engine* e);

@@ -62,6 +62,20 @@ class LbmAdjointResult(ctypes.Structure):
     ]
 
 
+class LbmOpening(ctypes.Structure):
+    _fields_ = [
+        ("outlet", ctypes.c_int32), ("axis", ctypes.c_int32), ("coordinate", ctypes.c_double),
+        ("normal", ctypes.c_double * 3), ("range", (ctypes.c_double * 2) * 3),
+    ]
+
+
+class LbmVoxelDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_triangles", ctypes.c_int64), ("triangles", _f64p), ("grid_size", ctypes.c_double),
+        ("n_openings", ctypes.c_int32), ("openings", ctypes.POINTER(LbmOpening)), ("device", ctypes.c_int32),
+    ]
+
+
 class LbmError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__("lbm error %d: %s" % (code, msg))
@@ -97,6 +111,12 @@ SIGNATURES = {
     "lbm_get_info": (ctypes.c_int, [_E, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),
     "lbm_adjoint_run": (ctypes.c_int, [_E, ctypes.POINTER(LbmAdjointDesc), ctypes.c_int32,
                                        ctypes.POINTER(LbmAdjointResult)]),
+    "lbm_stl_read_ascii": (ctypes.c_int, [ctypes.c_char_p, _i64p, ctypes.POINTER(_f64p)]),
+    "lbm_free": (None, [ctypes.c_void_p]),
+    "lbm_voxelise": (ctypes.c_int, [ctypes.POINTER(LbmVoxelDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "lbm_voxel_info": (ctypes.c_int, [_E, _i32p, _f64p, _f64p, _i64p, _i64p, _f64p]),
+    "lbm_voxel_describe": (ctypes.c_int, [_E, ctypes.POINTER(LbmDesc)]),
+    "lbm_voxel_destroy": (ctypes.c_int, [_E]),
     "lbm_last_error": (ctypes.c_char_p, [_E]),
 }
 

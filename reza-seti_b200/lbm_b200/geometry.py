@@ -429,3 +429,86 @@ def inlet_disc_profile(topo, mean, radius=None):
     R = float(topo["radius"][0]) if radius is None else radius
     v = np.maximum(0.0, 2.0 * mean * (1.0 - r2 / (R * R)))
     return v[:, None] * (-nrm)[None, :]
+
+
+# ----------------------------------------------------------- STL pipeline ---
+def read_stl(path):
+    """Triangles of an ASCII STL as [n, 12] (vertex 1, 2, 3, facet normal),
+    read by the library with the reference reader's line grammar."""
+    import ctypes
+
+    from . import capi
+    n = ctypes.c_int64()
+    buf = ctypes.POINTER(ctypes.c_double)()
+    capi.check(capi.lib().lbm_stl_read_ascii(str(path).encode(), ctypes.byref(n), ctypes.byref(buf)))
+    try:
+        return np.ctypeslib.as_array(buf, shape=(max(n.value, 1) * 12,))[: n.value * 12].reshape(-1, 12).copy()
+    finally:
+        capi.lib().lbm_free(buf)
+
+
+def opening(kind, plane, coordinate, normal, range_x=None, range_y=None, range_z=None):
+    """One inlet or outlet block of the reference's config.txt."""
+    return {"kind": kind, "plane": plane, "coordinate": float(coordinate), "normal": list(map(float, normal)),
+            "range_x": range_x, "range_y": range_y, "range_z": range_z}
+
+
+def voxelise_stl(triangles, grid_size, openings, device=0, info=False):
+    """Node set of an STL surface on the GPU (lbm_voxelise), as a topology dict
+    with the reference's classification; coordinates are grid indices.
+    `openings`: list of opening(...) dicts, inlets and outlets in config
+    order. With info, also returns (dims, origin, spacing, build_ms)."""
+    import ctypes
+
+    from . import capi
+    tris = np.ascontiguousarray(triangles, dtype=np.float64).reshape(-1, 12)
+    ops = (capi.LbmOpening * max(1, len(openings)))()
+    for o, b in zip(ops, openings):
+        o.outlet = 1 if b["kind"] == "outlet" else 0
+        o.axis = "xyz".index(b["plane"])
+        o.coordinate = b["coordinate"]
+        for a in range(3):
+            o.normal[a] = b["normal"][a]
+            r = b.get("range_" + "xyz"[a])
+            o.range[a][0], o.range[a][1] = (r[0], r[1]) if r is not None else (-np.inf, np.inf)
+    d = capi.LbmVoxelDesc()
+    d.n_triangles = len(tris)
+    d.triangles = tris.ctypes.data_as(capi._f64p)
+    d.grid_size = float(grid_size)
+    d.n_openings = len(openings)
+    d.openings = ops
+    d.device = device
+    v = ctypes.c_void_p()
+    L = capi.lib()
+    capi.check(L.lbm_voxelise(ctypes.byref(d), ctypes.byref(v)))
+    try:
+        desc = capi.LbmDesc()
+        capi.check(L.lbm_voxel_describe(v, ctypes.byref(desc)))
+        n = desc.n_nodes
+
+        def arr(ptr, count, dtype, shape=None):
+            a = np.ctypeslib.as_array(ptr, shape=(max(count, 1),))[:count].astype(dtype)
+            return a.reshape(shape) if shape else a
+
+        topo = {"coords": arr(desc.coords, 3 * n, np.int32, (n, 3)), "kind": arr(desc.kind, n, np.uint8),
+                "inlet": arr(desc.inlet, desc.n_inlet, np.int64),
+                "inlet_normal": np.array(list(desc.inlet_normal)),
+                "wall": arr(desc.wall, desc.n_wall, np.int64),
+                "nearwall": arr(desc.nearwall, desc.n_nearwall, np.int64),
+                "nearwall_normal": arr(desc.nearwall_normals, 3 * desc.n_nearwall, np.float64,
+                                       (desc.n_nearwall, 3))}
+        off = arr(desc.outlet_offsets, desc.n_outlets + 1, np.int64)
+        nodes = arr(desc.outlet_nodes, int(off[-1]) if len(off) else 0, np.int64)
+        normals = arr(desc.outlet_normals, 3 * desc.n_outlets, np.float64, (max(desc.n_outlets, 0), 3))
+        for k in range(desc.n_outlets):
+            topo["outlet_%d" % k] = nodes[off[k]:off[k + 1]]
+            topo["outlet_normal_%d" % k] = normals[k]
+        if info:
+            dims = (ctypes.c_int32 * 3)()
+            origin = (ctypes.c_double * 3)()
+            sp, ms = ctypes.c_double(), ctypes.c_double()
+            capi.check(L.lbm_voxel_info(v, dims, origin, ctypes.byref(sp), None, None, ctypes.byref(ms)))
+            return topo, (tuple(dims), tuple(origin), sp.value, ms.value)
+        return topo
+    finally:
+        L.lbm_voxel_destroy(v)

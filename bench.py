@@ -287,6 +287,9 @@ def run_gpu(args):
     configs = None
     if rank == 0 and not args.no_configs:
         configs = run_configs(torch, device)
+    voxel = None
+    if rank == 0 and not args.no_voxel:
+        voxel = run_voxel(torch, device)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -309,7 +312,7 @@ def run_gpu(args):
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": 2 * args.steps, "clocks": clocks, "device_flags": flags,
-            "variants": variants, "precision": precision, "adjoint": adjoint, "configs": configs,
+            "variants": variants, "precision": precision, "adjoint": adjoint, "configs": configs, "geometry_setup": voxel,
         }
         print(json.dumps(line))
     if dist:
@@ -546,6 +549,79 @@ def run_configs(torch, device):
     return out
 
 
+# -------------------------------------------------------- geometry setup ---
+def write_stl_ascii(path, tris):
+    with open(path, "w") as fh:
+        fh.write("solid vessel\n")
+        for t in tris:
+            fh.write("facet normal %.17g %.17g %.17g\nouter loop\n" % tuple(t[9:12]))
+            for v in range(3):
+                fh.write("vertex %.17g %.17g %.17g\n" % tuple(t[3 * v:3 * v + 3]))
+            fh.write("endloop\nendfacet\n")
+        fh.write("endsolid vessel\n")
+
+
+def write_reference_config(path, grid_size, length):
+    """config.txt of the reference (LBM.h parser) for a tube along z with the
+    inlet plane z = 0 and the outlet plane z = length."""
+    lines = ["parameters:", "", '  stl_file: "geom.stl"', '  FlowType: "Constant"', "  time_resolution: 1e-05",
+             "  density: 1060", "  kinematic_viscosity: 3.5e-6", "  relaxation_factor: 0.8",
+             "  grid_size: %r" % grid_size, "  pressure: 1", "  CteVel: 0.05", "  reynolds_number: 100",
+             "  number_of_outlets: 1", "  MaxIter: 1", "  IterToWrite: 1000000", "  Systole: 0.15",
+             "  Diastole: 0.9", "  period: 0.9", "  NumCycle: 1", "", "",
+             "inlets:", "", "    plane: z", "    coordinate: 0.0", "    normal: [0.0, 0.0, -1.0]", "", "",
+             "outlets:", "", "    plane: z", "    coordinate: %r" % float(length), "    normal: [0.0, 0.0, 1.0]", "",
+             "", "equations:", "    InletVel1: [0]", ""]
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines))
+
+
+def run_voxel(torch, device):
+    """Geometry setup from an STL: the GPU pipeline (lbm_voxelise) against the
+    reference's own Geometry + SubDomain construction (oracle/_ref/refharness,
+    stl mode, setup only) on the R = 16 pipe STL, and the GPU pipeline alone on
+    a triangulated radius-20 tortuous vessel (the reference needs hours)."""
+    from lbm_b200 import geometry as G
+    out = {}
+    # R = 16, L = 128 pipe, 64 x 32 facets, grid_size 0.5 (spacing 1)
+    tris = G.tube_triangles(lambda z: (0.37, 0.21), lambda z: 16.0, 0.0, 128.0, 64, 32)
+    ops = [G.opening("inlet", "z", 0.0, (0, 0, -1)), G.opening("outlet", "z", 128.0, (0, 0, 1))]
+    G.voxelise_stl(tris, 0.5, ops, device=device)  # warm-up (context, module load)
+    t0 = time.perf_counter()
+    topo, (dims, origin, sp, ms) = G.voxelise_stl(tris, 0.5, ops, device=device, info=True)
+    wall = time.perf_counter() - t0
+    pipe = {"triangles": len(tris), "grid_points": int(np.prod(dims)), "nodes": len(topo["kind"]),
+            "near_wall_nodes": len(topo["nearwall"]), "gpu_seconds": round(wall, 4)}
+    harness = os.path.join(ROOT, "oracle", "_ref", "refharness")
+    if os.path.exists(harness):
+        with tempfile.TemporaryDirectory() as tmp:
+            write_stl_ascii(os.path.join(tmp, "geom.stl"), tris)
+            write_reference_config(os.path.join(tmp, "config.txt"), 0.5, 128.0)
+            r = subprocess.run([harness, "stl", os.path.join(tmp, "config.txt"), "0", os.path.join(tmp, "d.bin"),
+                                "--time"], capture_output=True, text=True, timeout=1800)
+            try:
+                rep = json.loads(r.stdout.strip().splitlines()[-1])
+                pipe["reference_setup_seconds"] = rep["setup_seconds"]
+                pipe["reference_nodes"] = int(rep["nodes"])
+                pipe["speedup"] = round(rep["setup_seconds"] / wall, 1)
+            except (ValueError, IndexError, KeyError):
+                pipe["reference_setup_seconds"] = None
+    out["pipe16"] = pipe
+    # radius-20 tortuous stenosed vessel as an STL: 128 x 1024 facets
+    A, lam, R, Z = 30.0, 200.0, 20.0, 1024.0
+    tris = G.tube_triangles(lambda z: (256.37 + A * math.sin(2 * math.pi * z / lam), 256.21),
+                            lambda z: R * math.sqrt(1 - 0.5 * math.exp(-((z - Z / 2) ** 2) / (2 * (2 * R) ** 2))),
+                            0.0, Z, 128, 1024)
+    ops = [G.opening("inlet", "z", 0.0, (0, 0, -1)), G.opening("outlet", "z", Z, (0, 0, 1))]
+    t0 = time.perf_counter()
+    topo, (dims, origin, sp, ms) = G.voxelise_stl(tris, 0.5, ops, device=device, info=True)
+    wall = time.perf_counter() - t0
+    out["tortuous_R20"] = {"triangles": len(tris), "grid": list(dims), "grid_points": int(np.prod(dims)),
+                           "nodes": len(topo["kind"]), "near_wall_nodes": len(topo["nearwall"]),
+                           "gpu_seconds": round(wall, 3)}
+    return out
+
+
 # ----------------------------------------------------------------- adjoint ---
 ADJ_STEPS, ADJ_K, ADJ_TAU = 3000, 100, 0.6
 
@@ -747,7 +823,8 @@ def main():
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
-    ap.add_argument("--section", default="all", choices=["all", "precision", "adjoint", "configs"],
+    ap.add_argument("--no-voxel", action="store_true")
+    ap.add_argument("--section", default="all", choices=["all", "precision", "adjoint", "configs", "voxel"],
                     help="run only the precision study, the adjoint measurement or the branching/aneurysm runs")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -757,7 +834,8 @@ def main():
     elif args.section != "all":
         import torch
         torch.cuda.set_device(0)
-        run = {"precision": run_precision, "adjoint": run_adjoint, "configs": run_configs}[args.section]
+        run = {"precision": run_precision, "adjoint": run_adjoint, "configs": run_configs,
+               "voxel": run_voxel}[args.section]
         res = run(torch, 0)
         print(json.dumps({"section": args.section, **res}))
     else:

@@ -512,3 +512,44 @@ def voxelise_stl(triangles, grid_size, openings, device=0, info=False):
         return topo
     finally:
         L.lbm_voxel_destroy(v)
+
+
+def tube_triangles(center_fn, radius_fn, z0, z1, n_az, n_ax, phase=0.5):
+    """Closed triangulated tube around a centerline (x_c(z), y_c(z)) from z0 to
+    z1: rings of n_az vertices in the planes of n_ax + 1 stations (azimuthal
+    phase in facets, so that no vertex or edge sits on a lattice line), side
+    quads split in two, fan caps. Returns [n, 12] (vertices, outward facet
+    normal), the layout of lbm_voxel_desc.triangles."""
+    zs = np.linspace(z0, z1, n_ax + 1)
+    th = 2 * np.pi * (np.arange(n_az) + phase) / n_az
+    cen = np.array([center_fn(z) for z in zs])                     # [S, 2]
+    rad = np.array([radius_fn(z) for z in zs])                      # [S]
+    ring = np.empty((n_ax + 1, n_az, 3))
+    ring[..., 0] = cen[:, None, 0] + rad[:, None] * np.cos(th)[None, :]
+    ring[..., 1] = cen[:, None, 1] + rad[:, None] * np.sin(th)[None, :]
+    ring[..., 2] = zs[:, None]
+    a = np.arange(n_az)
+    b = (a + 1) % n_az
+    lo, hi = ring[:-1], ring[1:]
+    # two triangles per quad: (lo a, lo b, hi b), (lo a, hi b, hi a)
+    t1 = np.stack([lo[:, a], lo[:, b], hi[:, b]], axis=2).reshape(-1, 3, 3)
+    t2 = np.stack([lo[:, a], hi[:, b], hi[:, a]], axis=2).reshape(-1, 3, 3)
+    side = np.concatenate([t1, t2])
+    mid_c = np.concatenate([np.repeat(0.5 * (cen[:-1] + cen[1:]), n_az, axis=0)] * 2)
+    out_side = side.mean(axis=1)
+    out_side[:, :2] -= mid_c
+    out_side[:, 2] = 0.0
+    caps = []
+    outs = []
+    for k, sign in ((0, -1.0), (n_ax, 1.0)):
+        ctr = np.array([cen[k, 0], cen[k, 1], zs[k]])
+        caps.append(np.stack([np.broadcast_to(ctr, (n_az, 3)), ring[k, a], ring[k, b]], axis=1))
+        outs.append(np.broadcast_to(np.array([0.0, 0.0, sign]), (n_az, 3)))
+    tri = np.concatenate([side] + caps)
+    out = np.concatenate([out_side] + outs)
+    n = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    flip = (n * out).sum(axis=1) < 0
+    tri[flip] = tri[flip][:, [0, 2, 1]]
+    n[flip] = -n[flip]
+    return np.concatenate([tri.reshape(-1, 9), n], axis=1)

@@ -311,6 +311,33 @@ int lbm_voxel_info(const lbm_voxel* v, int32_t dims[3], double origin[3], double
 int lbm_voxel_describe(const lbm_voxel* v, lbm_desc* desc);
 int lbm_voxel_destroy(lbm_voxel* v);
 
+/* ------------------------------------------------------- result files ---
+ * The files of Simulation::WriteOutput (Simulation.cpp:835-856) without VTK.
+ * Errors: lbm_last_error(NULL) for file problems, lbm_last_error(e) for an
+ * engine state problem (state of the last step not observed). */
+
+/* OutputFile::WriteSurfaceAttribute (OutputFile.cpp:234-316): one row per
+ * near-wall node, in the near-wall list's order: X,Y,Z (origin + index x
+ * spacing, as Geometry::pointsBox), WSS, with pulsatile != 0 also OSI and
+ * TAWSS, and |u|; the reference's header line and ostream number format. */
+int lbm_write_surface_csv(lbm_engine* e, const char* path, const double origin[3], double spacing,
+                          int32_t pulsatile);
+
+/* OutputFile::processFlowData (OutputFile.cpp:395-483): reads such a file and
+ * writes it with WSS (and OSI, TAWSS) replaced by the mean over the other
+ * rows within `radius` (the row's own value when there is none). The
+ * neighbour search runs on `device`; neighbour sets and summation order are
+ * the reference's, so the numbers written are the same. */
+int lbm_smooth_surface_csv(const char* in_path, const char* out_path, double radius, int32_t pulsatile,
+                           int32_t device);
+
+/* OutputFile::WriteVTK_Collective (OutputFile.cpp:60-230) as VTK XML with raw
+ * appended data: every node (order: z, then y, x fastest) with Velocity,
+ * Density, VelocityMagnitude, and a hexahedron for each lattice cell (x, y, z)
+ * with x < cells[0] - 1, y < cells[1] - 1, z < cells[2] - 1 whose eight
+ * corners are nodes; cells = the reference's Geometry nx, ny, nz. */
+int lbm_write_vtu(lbm_engine* e, const char* path, const int32_t cells[3]);
+
 /* Message of the last failed call on e (or of the last failed lbm_create when
  * e is NULL). Never NULL. */
 const char* lbm_last_error(const lbm_engine* e);

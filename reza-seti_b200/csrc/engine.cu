@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "adjoint.h"
+#include "engine_view.h"
 #include "errors.h"
 #include "lbm_b200.h"
 #include "launch.h"
@@ -339,6 +340,9 @@ struct lbm_engine {
     double wave_period = 1.0;
     std::vector<double> wave_amp, wave_phase;
     int* perm = nullptr;
+    // host copies for the result writers: caller-order coordinates, near-wall list
+    std::vector<int32_t> host_coords;
+    std::vector<int64_t> host_nearwall;
     long long* flux_nodes = nullptr;  // internal indices: the inlet list, then the outlet lists
     double* flux_partials = nullptr;
     double* flux_out = nullptr;
@@ -731,6 +735,8 @@ int create(const lbm_desc* d, lbm_engine** out) {
         delete e;
         return LBM_ERR_ARGUMENT;
     }
+    e->host_coords.assign(d->coords, d->coords + 3 * d->n_nodes);
+    if (d->n_nearwall > 0) e->host_nearwall.assign(d->nearwall, d->nearwall + d->n_nearwall);
     auto bail = [&](cudaError_t ce, const char* where) {
         g_create_error = std::string(where) + ": " + cudaGetErrorString(ce);
         lbm_destroy(e);
@@ -1154,3 +1160,17 @@ void lbm::set_global_error(const std::string& msg) { g_create_error = msg; }
 extern "C" {
 
 }  // extern "C"
+
+namespace lbm {
+// Caller-order node coordinates and near-wall list of an engine, for the
+// result writers (output.cu).
+bool engine_view(const lbm_engine* e, EngineView& v) {
+    if (!e) return false;
+    v.n = (int64_t)(e->host_coords.size() / 3);
+    v.coords = e->host_coords.data();
+    v.n_nw = (int64_t)e->host_nearwall.size();
+    v.nearwall = e->host_nearwall.data();
+    v.Q = e->Q;
+    return true;
+}
+}  // namespace lbm

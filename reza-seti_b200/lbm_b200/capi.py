@@ -117,6 +117,10 @@ SIGNATURES = {
     "lbm_voxel_info": (ctypes.c_int, [_E, _i32p, _f64p, _f64p, _i64p, _i64p, _f64p]),
     "lbm_voxel_describe": (ctypes.c_int, [_E, ctypes.POINTER(LbmDesc)]),
     "lbm_voxel_destroy": (ctypes.c_int, [_E]),
+    "lbm_write_surface_csv": (ctypes.c_int, [_E, ctypes.c_char_p, _f64p, ctypes.c_double, ctypes.c_int32]),
+    "lbm_smooth_surface_csv": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int32,
+                                              ctypes.c_int32]),
+    "lbm_write_vtu": (ctypes.c_int, [_E, ctypes.c_char_p, _i32p]),
     "lbm_last_error": (ctypes.c_char_p, [_E]),
 }
 

@@ -215,6 +215,18 @@ class Engine:
             out["populations"] = fp
         return out
 
+    def write_surface_csv(self, path, origin=(0.0, 0.0, 0.0), spacing=1.0, pulsatile=False):
+        """The reference's <iter>_FlowHemodynamics.csv (lbm_write_surface_csv)."""
+        o = np.ascontiguousarray(origin, dtype=np.float64)
+        self._check(capi.lib().lbm_write_surface_csv(self._h, str(path).encode(), _p(o, capi._f64p),
+                                                     float(spacing), int(bool(pulsatile))))
+
+    def write_vtu(self, path, cells):
+        """The reference's Fluid_Variables/<k>.vtu content (lbm_write_vtu);
+        cells = the reference grid's interval counts (nx, ny, nz)."""
+        c = np.ascontiguousarray(cells, dtype=np.int32)
+        self._check(capi.lib().lbm_write_vtu(self._h, str(path).encode(), _p(c, capi._i32p)))
+
     def info(self):
         vals = [ctypes.c_int64() for _ in range(6)]
         self._check(capi.lib().lbm_get_info(self._h, *[ctypes.byref(v) for v in vals]))
@@ -267,3 +279,10 @@ class Simulation:
                 t += float(p["dt"])
                 n += 1
             self.engine.step(n)
+
+
+def smooth_surface_csv(in_path, out_path, radius=0.25, pulsatile=False, device=0):
+    """The reference's FlowHemodynamics/<phase>_<iter>_FlowHemodynamics.csv
+    (lbm_smooth_surface_csv; search radius 0.25 in Simulation::WriteOutput)."""
+    capi.check(capi.lib().lbm_smooth_surface_csv(str(in_path).encode(), str(out_path).encode(), float(radius),
+                                                 int(bool(pulsatile)), int(device)))

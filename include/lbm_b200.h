@@ -338,6 +338,92 @@ int lbm_smooth_surface_csv(const char* in_path, const char* out_path, double rad
  * corners are nodes; cells = the reference's Geometry nx, ny, nz. */
 int lbm_write_vtu(lbm_engine* e, const char* path, const int32_t cells[3]);
 
+/* ------------------------------------------------- pulsatile waveform ---
+ * The inlet waveform of Simulation::getInletVelocity (Simulation.cpp:519-534)
+ * with its polynomials given instead of fixed (pulsatile.h:55-69 hard-codes
+ * the three pieces that config.txt's equations: section lists, and the
+ * reference never reads that section). With x = fmod(t, period), piece k
+ * applies where bounds[k] * period <= x < bounds[k + 1] * period, and its value
+ * is c_0 x^d + c_1 x^(d-1) + ... + c_d, summed left to right with the
+ * reference's powers (pow, x * x for the square, x, 1); outside every piece
+ * the value is 0. The reference's pieces (bounds 0, 0.1, 0.3, 0.9 of a 0.9 s
+ * period with its coefficients) give its waveform bit for bit. */
+typedef struct {
+    double period;            /* Pulsatile::period */
+    int32_t n_pieces;
+    const double* bounds;     /* [n_pieces + 1], fractions of the period, ascending */
+    const int32_t* n_coeffs;  /* [n_pieces], 1..LBM_PULSE_MAX_COEFFS */
+    const double* coeffs;     /* concatenated, highest power first (the equations: order) */
+} lbm_pulse_desc;
+
+#define LBM_PULSE_MAX_COEFFS 16
+
+/* Uses w for pulsatile flow from the next step on; NULL restores the
+ * reference's built-in waveform. */
+int lbm_set_pulsatile(lbm_engine* e, const lbm_pulse_desc* w);
+
+/* The waveform value at time t (host only; w NULL: the reference's).
+ * Errors: lbm_last_error(NULL). */
+int lbm_pulse_eval(const lbm_pulse_desc* w, double t, double* value);
+
+/* ------------------------------------------------------------ config.txt ---
+ * parseInputFile (LBM.h:81-188) with its line grammar: " \t"-trimmed lines,
+ * '#' lines skipped, "name:" opens a section; in parameters: key: value
+ * (numbers through std::stod / std::stoi, quotes removed from FlowType and
+ * stl_file); in inlets / outlets: blocks of plane, coordinate, range_x/y/z
+ * and normal lines ended by an empty line (missing ranges are unbounded); in
+ * equations: "name: [c0, c1, ...]". Where the reference reads an
+ * uninitialised value or indexes past a vector (a block without coordinate
+ * or normal, a range with fewer than two values), or a plane other than x,
+ * y, z, this parser returns LBM_ERR_ARGUMENT instead.
+ *
+ * Extension keys in parameters: (the reference's parser skips unknown keys,
+ * so a file carrying them still runs there): lattice (D3Q19 | D3Q27, the
+ * compile-time choice of Macro.h:49), storage (f64 | f32 | f16 | bf16),
+ * boundary (reference | physics), period (of the pulsatile waveform; the
+ * reference's file carries it but its parser ignores it and uses 0.9),
+ * equation_bounds ([fractions of the period], one more than equations),
+ * outlet_density, harmonic_period_steps, harmonic_amplitudes [...],
+ * harmonic_phases [...] (FlowType "Harmonic"), device. */
+#define LBM_CONFIG_MAX_OPENINGS 64
+#define LBM_CONFIG_MAX_EQUATIONS 16
+#define LBM_CONFIG_MAX_HARMONICS 16
+
+typedef struct {
+    char name[64];
+    int32_t n_coeffs;
+    double coeffs[LBM_PULSE_MAX_COEFFS];
+} lbm_equation;
+
+typedef struct {
+    /* SimulationParameters (SimulationParameters.h:51-67) */
+    char stl_file[1024];
+    char flow_type[64];
+    double dt, rho, nu_blood, tau, grid_size, pressure, cte_vel, reynolds_number, systole, diastole;
+    int32_t number_of_outlets, max_iter, iter_to_write, num_cycle;
+    int32_t n_inlets, n_outlets;
+    lbm_opening openings[LBM_CONFIG_MAX_OPENINGS]; /* inlets, then outlets, each in file order */
+    int32_t n_equations;
+    lbm_equation equations[LBM_CONFIG_MAX_EQUATIONS];
+    /* extensions and what follows from them */
+    int32_t flow;             /* lbm_flow of FlowType (Constant, Pulsatile, Harmonic), -1 for others */
+    int32_t lattice;          /* lbm_lattice, default D3Q19 */
+    int32_t storage;          /* lbm_storage, default F64 */
+    int32_t bc_mode;          /* lbm_bc_mode, default REFERENCE */
+    int32_t device;           /* default 0 */
+    double period;            /* default 0.9 */
+    int32_t n_bounds;         /* 0: the reference's 0, 0.1, 0.3, 0.9 for three equations */
+    double equation_bounds[LBM_CONFIG_MAX_EQUATIONS + 1];
+    double outlet_density;    /* default 1 */
+    double harmonic_period_steps;
+    int32_t n_harmonics;
+    double harmonic_amplitudes[LBM_CONFIG_MAX_HARMONICS];
+    double harmonic_phases[LBM_CONFIG_MAX_HARMONICS];
+} lbm_config;
+
+/* Errors: lbm_last_error(NULL). */
+int lbm_config_parse(const char* path, lbm_config* out);
+
 /* Message of the last failed call on e (or of the last failed lbm_create when
  * e is NULL). Never NULL. */
 const char* lbm_last_error(const lbm_engine* e);

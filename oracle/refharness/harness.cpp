@@ -26,9 +26,18 @@
  *   are left out. With --iterate the reference's own Iterate() runs instead
  *   (output goes through the no-op OutputFile).
  *
+ * Config
+ *   config <config.txt>: runs the reference's parseInputFile (LBM.h:81-188)
+ *   and prints what it read, one item per line ("key value", doubles with 17
+ *   significant digits; "inlet"/"outlet" lines: plane, coordinate, then each
+ *   range's values and the normal's, each list prefixed by its length;
+ *   "equation" lines: name, count, coefficients). Parse errors print
+ *   "error <what>" and exit 3.
+ *
  * Usage
  *   refharness stl <config> <steps> <out.bin> [--phases] [--time] [--iterate]
  *   refharness nodemap <config> <map.bin> <steps> <out.bin> [--phases] [--time]
+ *   refharness config <config>
  *   <out.bin> may be "-" for no dump (timing runs).
  */
 #include <array>
@@ -339,13 +348,55 @@ int usage() {
     std::fprintf(stderr,
                  "usage: refharness stl <config> <steps> <out.bin> [--phases] [--time] [--iterate]\n"
                  "       refharness nodemap <config> <map.bin> <steps> <out.bin> [--phases] "
-                 "[--time]\n");
+                 "[--time]\n"
+                 "       refharness config <config>\n");
     return 2;
+}
+
+void print_list(const std::vector<double>& v) {
+    std::printf(" %zu", v.size());
+    for (double x : v) std::printf(" %.17g", x);
+}
+
+int print_config(const std::string& path) {
+    SimulationParameters sp;
+    try {
+        parseInputFile(path, sp);
+    } catch (const std::exception& ex) {
+        std::printf("error %s\n", ex.what());
+        return 3;
+    }
+    std::printf("stl_file %s\n", sp.stlFile.c_str());
+    std::printf("FlowType %s\n", sp.FlowType.c_str());
+    std::printf("dt %.17g\nrho %.17g\nnu_blood %.17g\ntau %.17g\ngrid_size %.17g\npressure %.17g\n", sp.dt,
+                sp.rho, sp.nu_blood, sp.tau, sp.dx, sp.pressure);
+    std::printf("CteVel %.17g\nreynolds_number %.17g\nSystole %.17g\nDiastole %.17g\n", sp.CteVel,
+                sp.reynoldsNumber, sp.Systole, sp.Diastole);
+    std::printf("number_of_outlets %d\nMaxIter %d\nIterToWrite %d\nNumCycle %d\n", sp.num_Out, sp.MaxIter,
+                sp.IterToWrite, (int)sp.NumCycle);
+    auto opening = [](const char* kind, const std::string& plane, double coordinate, const std::vector<double>& rx,
+                      const std::vector<double>& ry, const std::vector<double>& rz, const std::vector<double>& n) {
+        std::printf("%s %s %.17g", kind, plane.c_str(), coordinate);
+        print_list(rx);
+        print_list(ry);
+        print_list(rz);
+        print_list(n);
+        std::printf("\n");
+    };
+    for (const auto& o : sp.inlets) opening("inlet", o.plane, o.coordinate, o.range_x, o.range_y, o.range_z, o.normal);
+    for (const auto& o : sp.outlets) opening("outlet", o.plane, o.coordinate, o.range_x, o.range_y, o.range_z, o.normal);
+    for (const auto& q : sp.equations) {
+        std::printf("equation %s", q.name.c_str());
+        print_list(q.coeffs);
+        std::printf("\n");
+    }
+    return 0;
 }
 
 }  // namespace
 
 int main(int argc, char** argv) {
+    if (argc == 3 && std::string(argv[1]) == "config") return print_config(argv[2]);
     if (argc < 5) return usage();
     const std::string mode = argv[1];
     std::string config = argv[2], mappath, out;

@@ -27,6 +27,7 @@
 #include "engine_view.h"
 #include "errors.h"
 #include "lbm_b200.h"
+#include "pulse.h"
 #include "launch.h"
 #include "reduce.cuh"
 
@@ -300,6 +301,8 @@ struct lbm_engine {
     double tau = 1, omega = 1, dt = 0, spacing = 1, wss_c = 0;
     double inlet_normal[3] = {0, 0, 0};
     int flow = LBM_FLOW_CONSTANT;
+    bool pulse_custom = false;  // lbm_set_pulsatile pieces instead of the reference's
+    lbm::Pulse pulse;
     double cte_vel = 0.0, out_rho = 1.0;
     int64_t step = 0;
     double runtime = 0.0;
@@ -464,11 +467,17 @@ OpenArgs<S, Q> open_args(lbm_engine* e, double scale) {
     return o;
 }
 
+// Pulsatile inlet velocity at flow clock t: the reference's waveform, or the
+// pieces given with lbm_set_pulsatile.
+double pulsatile_at(const lbm_engine* e, double t) {
+    return e->pulse_custom ? lbm::pulse_value(e->pulse, t) : pulsatile_velocity(t, 0.9);
+}
+
 // Inlet waveform factor of step k (0-based) whose flow clock reads runtime_k:
 // 1 for constant flow, the reference waveform value for pulsatile flow, the
 // harmonic factor for harmonic flow.
 double inlet_factor(const lbm_engine* e, int64_t k, double runtime_k) {
-    if (e->flow == LBM_FLOW_PULSATILE) return pulsatile_velocity(runtime_k, 0.9);
+    if (e->flow == LBM_FLOW_PULSATILE) return pulsatile_at(e, runtime_k);
     double f = 1.0;
     if (e->flow == LBM_FLOW_HARMONIC) {
         const double two_pi = 6.283185307179586;
@@ -602,7 +611,7 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
         const int64_t t = e->step + 1;
         const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
         // reference-mode inlet velocity of this step (Simulation.cpp:558-562)
-        const double vel = pulsatile ? pulsatile_velocity(e->runtime, 0.9)
+        const double vel = pulsatile ? pulsatile_at(e, e->runtime)
                                      : e->cte_vel * inlet_factor(e, e->step, e->runtime);
         int obs = 0;
         if (e->observe && i >= n_steps - 2) obs |= 2;
@@ -867,6 +876,20 @@ static int reapply_initial_store(lbm_engine* e) {
     cudaSetDevice(e->device);
     if (int rc = init_from_obs(e)) return rc;
     return sync(e);
+}
+
+int lbm_set_pulsatile(lbm_engine* e, const lbm_pulse_desc* w) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    if (!w) {
+        e->pulse_custom = false;
+        return LBM_OK;
+    }
+    lbm::Pulse p;
+    const std::string err = lbm::pulse_from_desc(*w, p);
+    if (!err.empty()) return e->fail(LBM_ERR_ARGUMENT, err);
+    e->pulse = std::move(p);
+    e->pulse_custom = true;
+    return LBM_OK;
 }
 
 int lbm_set_waveform(lbm_engine* e, double period_steps, int32_t n_harmonics, const double* amplitude,

@@ -60,13 +60,78 @@ void check(int rc, lbm_engine* e, const char* what) {
     }
 }
 
-int storage_from_env() {
+// Storage type: LBM_B200_STORAGE if set, else the config's storage key.
+int storage_from_env(int configured) {
     const char* s = std::getenv("LBM_B200_STORAGE");
-    if (!s || !std::strcmp(s, "f64")) return LBM_STORE_F64;
+    if (!s) return configured;
+    if (!std::strcmp(s, "f64")) return LBM_STORE_F64;
     if (!std::strcmp(s, "f32")) return LBM_STORE_F32;
     if (!std::strcmp(s, "f16")) return LBM_STORE_F16;
     if (!std::strcmp(s, "bf16")) return LBM_STORE_BF16;
-    return LBM_STORE_F64;
+    return configured;
+}
+
+// The extension keys of config.txt (lbm_config_parse on the file LBM.cpp's
+// main read, "config.txt" in the working directory). The drop-in links the
+// reference's D3Q19 SubDomain and reproduces its boundary rules, so it
+// accepts only lattice D3Q19 and boundary reference; physics mode and D3Q27
+// run through the library's own config runner. A file this parser rejects
+// (where the reference reads undefined values) leaves the defaults.
+lbm_config config_extensions() {
+    lbm_config c{};
+    c.lattice = LBM_D3Q19;
+    c.storage = LBM_STORE_F64;
+    c.bc_mode = LBM_BC_REFERENCE;
+    c.period = 0.9;
+    if (lbm_config_parse("config.txt", &c) != LBM_OK) {
+        std::cerr << "B200 engine: config.txt extensions not read: " << lbm_last_error(nullptr) << std::endl;
+        c = lbm_config{};
+        c.lattice = LBM_D3Q19;
+        c.storage = LBM_STORE_F64;
+        c.bc_mode = LBM_BC_REFERENCE;
+        c.period = 0.9;
+        return c;
+    }
+    if (c.lattice != LBM_D3Q19 || c.bc_mode != LBM_BC_REFERENCE) {
+        std::cerr << "B200 engine: the drop-in runs lattice D3Q19 with the reference's boundary rules; "
+                     "use the library's config runner for D3Q27 or physics boundaries"
+                  << std::endl;
+        std::exit(1);
+    }
+    return c;
+}
+
+// Pulsatile pieces from the config's equations: when they describe a whole
+// waveform (three equations, the reference's piece bounds; or as many as
+// equation_bounds has intervals). The reference parses equations: but its
+// waveform is fixed (pulsatile.h:55-69); with its own coefficients both agree.
+void set_waveform_from_equations(lbm_engine* e, const SimulationParameters& sp, const lbm_config& c) {
+    const size_t n = sp.equations.size();
+    if (n == 0) return;
+    for (const auto& q : sp.equations)
+        if (q.coeffs.empty() || q.coeffs.size() > LBM_PULSE_MAX_COEFFS) return;
+    std::vector<double> bounds;
+    if (c.n_bounds > 0) {
+        if ((size_t)c.n_bounds != n + 1) return;
+        bounds.assign(c.equation_bounds, c.equation_bounds + c.n_bounds);
+    } else if (n == 3) {
+        bounds = {0.0, 0.1, 0.3, 0.9};
+    } else {
+        return;
+    }
+    std::vector<int32_t> counts;
+    std::vector<double> coeffs;
+    for (const auto& q : sp.equations) {
+        counts.push_back((int32_t)q.coeffs.size());
+        coeffs.insert(coeffs.end(), q.coeffs.begin(), q.coeffs.end());
+    }
+    lbm_pulse_desc w{};
+    w.period = c.period;
+    w.n_pieces = (int32_t)n;
+    w.bounds = bounds.data();
+    w.n_coeffs = counts.data();
+    w.coeffs = coeffs.data();
+    check(lbm_set_pulsatile(e, &w), e, "lbm_set_pulsatile");
 }
 
 int kind_of(const Node& n) {
@@ -178,7 +243,8 @@ Simulation::Simulation(SubDomain& SubDomain, SimulationParameters& simParams) : 
 
     lbm_desc d{};
     d.lattice = _nLatNodes;
-    d.storage = storage_from_env();
+    const lbm_config ext = config_extensions();
+    d.storage = storage_from_env(ext.storage);
     d.bc_mode = LBM_BC_REFERENCE;
     d.device = 0;
     d.n_nodes = n;
@@ -201,6 +267,7 @@ Simulation::Simulation(SubDomain& SubDomain, SimulationParameters& simParams) : 
     d.dt = m_dt;
     d.spacing = SubDomain_.Geometry_.spacing;
     check(lbm_create(&d, &st.e), nullptr, "lbm_create");
+    if (simParams.FlowType == "Pulsatile") set_waveform_from_equations(st.e, simParams, ext);
     Iterate();
 }
 

@@ -85,6 +85,43 @@ class LbmError(RuntimeError):
 _lib = None
 
 # name -> (restype, argtypes); mirrors include/lbm_b200.h
+PULSE_MAX_COEFFS = 16
+CONFIG_MAX_OPENINGS = 64
+CONFIG_MAX_EQUATIONS = 16
+CONFIG_MAX_HARMONICS = 16
+
+
+class LbmPulseDesc(ctypes.Structure):
+    _fields_ = [
+        ("period", ctypes.c_double), ("n_pieces", ctypes.c_int32), ("bounds", _f64p),
+        ("n_coeffs", _i32p), ("coeffs", _f64p),
+    ]
+
+
+class LbmEquation(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 64), ("n_coeffs", ctypes.c_int32),
+                ("coeffs", ctypes.c_double * PULSE_MAX_COEFFS)]
+
+
+class LbmConfig(ctypes.Structure):
+    _fields_ = [
+        ("stl_file", ctypes.c_char * 1024), ("flow_type", ctypes.c_char * 64),
+        ("dt", ctypes.c_double), ("rho", ctypes.c_double), ("nu_blood", ctypes.c_double), ("tau", ctypes.c_double),
+        ("grid_size", ctypes.c_double), ("pressure", ctypes.c_double), ("cte_vel", ctypes.c_double),
+        ("reynolds_number", ctypes.c_double), ("systole", ctypes.c_double), ("diastole", ctypes.c_double),
+        ("number_of_outlets", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("iter_to_write", ctypes.c_int32),
+        ("num_cycle", ctypes.c_int32), ("n_inlets", ctypes.c_int32), ("n_outlets", ctypes.c_int32),
+        ("openings", LbmOpening * CONFIG_MAX_OPENINGS), ("n_equations", ctypes.c_int32),
+        ("equations", LbmEquation * CONFIG_MAX_EQUATIONS),
+        ("flow", ctypes.c_int32), ("lattice", ctypes.c_int32), ("storage", ctypes.c_int32),
+        ("bc_mode", ctypes.c_int32), ("device", ctypes.c_int32), ("period", ctypes.c_double),
+        ("n_bounds", ctypes.c_int32), ("equation_bounds", ctypes.c_double * (CONFIG_MAX_EQUATIONS + 1)),
+        ("outlet_density", ctypes.c_double), ("harmonic_period_steps", ctypes.c_double),
+        ("n_harmonics", ctypes.c_int32), ("harmonic_amplitudes", ctypes.c_double * CONFIG_MAX_HARMONICS),
+        ("harmonic_phases", ctypes.c_double * CONFIG_MAX_HARMONICS),
+    ]
+
+
 _E = ctypes.c_void_p
 SIGNATURES = {
     "lbm_create": (ctypes.c_int, [ctypes.POINTER(LbmDesc), ctypes.POINTER(ctypes.c_void_p)]),
@@ -121,6 +158,9 @@ SIGNATURES = {
     "lbm_smooth_surface_csv": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int32,
                                               ctypes.c_int32]),
     "lbm_write_vtu": (ctypes.c_int, [_E, ctypes.c_char_p, _i32p]),
+    "lbm_set_pulsatile": (ctypes.c_int, [_E, ctypes.POINTER(LbmPulseDesc)]),
+    "lbm_pulse_eval": (ctypes.c_int, [ctypes.POINTER(LbmPulseDesc), ctypes.c_double, _f64p]),
+    "lbm_config_parse": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(LbmConfig)]),
     "lbm_last_error": (ctypes.c_char_p, [_E]),
 }
 

@@ -117,6 +117,12 @@ class Engine:
         self._check(capi.lib().lbm_set_waveform(self._h, float(period_steps), len(a), _p(a, capi._f64p),
                                                 _p(p, capi._f64p)))
 
+    def set_pulsatile(self, pulse):
+        """Pulsatile waveform pieces (lbm_set_pulsatile): a config.Pulse, or
+        None for the reference's built-in waveform."""
+        self._pulse = pulse  # the descriptor's arrays must outlive the call only; kept for inspection
+        self._check(capi.lib().lbm_set_pulsatile(self._h, ctypes.byref(pulse.desc) if pulse is not None else None))
+
     def set_inlet_profile(self, vel):
         v = np.ascontiguousarray(vel, dtype=np.float64).reshape(self.n_inlet, 3)
         self._check(capi.lib().lbm_set_inlet_profile(self._h, _p(v, capi._f64p)))

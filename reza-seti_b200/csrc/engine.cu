@@ -326,8 +326,9 @@ struct lbm_engine {
     void* out_buf = nullptr;
     float* out_nrm = nullptr;
     int* nw_node = nullptr;
-    double* nw_normal = nullptr;
-    double* nw_mom = nullptr;
+    double* nw_normal = nullptr;   // FP64 normals (adjoint)
+    void* nw_normal_c = nullptr;   // normals in the compute type (wall shear stress)
+    void* nw_mom = nullptr;        // [n_nw][4] in the compute type
     void* nw_s = nullptr;
     double* wss = nullptr;
     double* acc = nullptr;
@@ -434,8 +435,8 @@ BoundaryArgs<S, Q> boundary_args(lbm_engine* e, double vel, bool with_wss, bool 
     b.n_wss = with_wss ? e->nw() : 0;
     b.n_nw = e->nw();
     b.nw_s = (const C*)e->nw_s;
-    b.nw_normal = e->nw_normal;
-    b.nw_mom = e->nw_mom;
+    b.nw_normal = (const C*)e->nw_normal_c;
+    b.nw_mom = (C*)e->nw_mom;
     b.wss = e->wss;
     b.acc = e->acc;
     b.accmag = e->accmag;
@@ -514,7 +515,7 @@ int init_from_obs(lbm_engine* e) {
     if (rc) return rc;
     if (int rc2 = open_pass(e, e->step, e->runtime)) return rc2;
     cudaError_t ce = launch_nearwall_moments(e->nw(), e->nw_node, e->obs_mom[mb], e->t.ld, e->shifted(),
-                                             e->nw_mom, e->stream);
+                                             e->nw_mom, e->storage != LBM_STORE_F64, e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "near-wall moments");
     e->phase = 1;
     e->wss_pending = false;
@@ -787,7 +788,17 @@ int create(const lbm_desc* d, lbm_engine** out) {
     e->out_buf = ob;
     if ((ce = e->upload(&e->nw_node, t.nw_node)) != cudaSuccess) return bail(ce, "near-wall");
     if ((ce = e->upload(&e->nw_normal, t.nw_normal)) != cudaSuccess) return bail(ce, "near-wall");
-    if ((ce = e->alloc(&e->nw_mom, (size_t)4 * std::max(1, e->nw()))) != cudaSuccess) return bail(ce, "near-wall");
+    if (celem == 8) {
+        e->nw_normal_c = e->nw_normal;
+    } else {
+        std::vector<float> nf(t.nw_normal.begin(), t.nw_normal.end());
+        float* d_nf = nullptr;
+        if ((ce = e->upload(&d_nf, nf)) != cudaSuccess) return bail(ce, "near-wall");
+        e->nw_normal_c = d_nf;
+    }
+    char* nwm = nullptr;
+    if ((ce = e->alloc(&nwm, (size_t)4 * std::max(1, e->nw()) * celem)) != cudaSuccess) return bail(ce, "near-wall");
+    e->nw_mom = nwm;
     char* nws = nullptr;
     if ((ce = e->alloc(&nws, (size_t)e->Q * std::max(1, e->nw()) * celem)) != cudaSuccess) return bail(ce, "near-wall");
     e->nw_s = nws;

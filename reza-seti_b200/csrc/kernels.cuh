@@ -127,8 +127,11 @@ struct BoundaryArgs {
     int n_wss;
     int n_nw;
     const C* nw_s;            // [Q][n_nw] arriving populations of the previous step
-    const double* nw_normal;  // [n_nw][3]
-    double* nw_mom;           // [n_nw][4] moments that step's f_eq used (rho or rho-1, u)
+    // normals and moments in the compute type: the FP32 traction reads both
+    // as float, and the moments it stores are FP32 values, so FP32 storage
+    // keeps them exactly in 28 instead of 56 bytes per node
+    const C* nw_normal;       // [n_nw][3]
+    C* nw_mom;                // [n_nw][4] moments that step's f_eq used (rho or rho-1, u)
     double* wss;              // [n_nw]
     double* acc;              // [n_nw][3]
     double* accmag;           // [n_nw]
@@ -412,8 +415,8 @@ __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
     C s[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) s[q] = a.nw_s[(long long)q * a.n_nw + k];
-    double* mom = a.nw_mom + 4 * (long long)k;
-    const double* nd = a.nw_normal + 3 * (long long)k;
+    C* mom = a.nw_mom + 4 * (long long)k;
+    const C* nd = a.nw_normal + 3 * (long long)k;
     double tau[3];
     if constexpr (sizeof(C) == 8) {
         // FP64: the reference's own triple loop, operand order kept
@@ -466,10 +469,10 @@ __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
     } else {
         moments_shifted<Q>(s, false, m0, u);
     }
-    mom[0] = (double)m0;
-    mom[1] = (double)u[0];
-    mom[2] = (double)u[1];
-    mom[3] = (double)u[2];
+    mom[0] = m0;
+    mom[1] = u[0];
+    mom[2] = u[1];
+    mom[3] = u[2];
 }
 
 // ---------------------------------------------------------------- kernels ---

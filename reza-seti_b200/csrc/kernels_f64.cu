@@ -19,22 +19,29 @@ cudaError_t launch_fill_weights(double* obs_pop, long long ld, int n, int q, cud
     return cudaGetLastError();
 }
 
-// Moments of the near-wall nodes from obs_mom, after initialisation.
+// Moments of the near-wall nodes from obs_mom, after initialisation, in the
+// compute type T of the wall shear stress pass.
+template <class T>
 __global__ void nearwall_moments_kernel(int n_nw, const int* nw_node, const double* obs_mom, long long ld,
-                                        bool shifted, double* nw_mom) {
+                                        bool shifted, T* nw_mom) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_nw) return;
     const int n = nw_node[i];
-    nw_mom[4 * (long long)i] = shifted ? obs_mom[n] - 1.0 : obs_mom[n];
-    nw_mom[4 * (long long)i + 1] = obs_mom[ld + n];
-    nw_mom[4 * (long long)i + 2] = obs_mom[2 * ld + n];
-    nw_mom[4 * (long long)i + 3] = obs_mom[3 * ld + n];
+    nw_mom[4 * (long long)i] = (T)(shifted ? obs_mom[n] - 1.0 : obs_mom[n]);
+    nw_mom[4 * (long long)i + 1] = (T)obs_mom[ld + n];
+    nw_mom[4 * (long long)i + 2] = (T)obs_mom[2 * ld + n];
+    nw_mom[4 * (long long)i + 3] = (T)obs_mom[3 * ld + n];
 }
 
 cudaError_t launch_nearwall_moments(int n_nw, const int* nw_node, const double* obs_mom, long long ld,
-                                    bool shifted, double* nw_mom, cudaStream_t st) {
+                                    bool shifted, void* nw_mom, bool narrow, cudaStream_t st) {
     if (n_nw == 0) return cudaSuccess;
-    nearwall_moments_kernel<<<(n_nw + 127) / 128, 128, 0, st>>>(n_nw, nw_node, obs_mom, ld, shifted, nw_mom);
+    if (narrow)
+        nearwall_moments_kernel<float><<<(n_nw + 127) / 128, 128, 0, st>>>(n_nw, nw_node, obs_mom, ld, shifted,
+                                                                            (float*)nw_mom);
+    else
+        nearwall_moments_kernel<double><<<(n_nw + 127) / 128, 128, 0, st>>>(n_nw, nw_node, obs_mom, ld, shifted,
+                                                                             (double*)nw_mom);
     return cudaGetLastError();
 }
 

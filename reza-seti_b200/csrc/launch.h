@@ -28,8 +28,10 @@ cudaError_t launch_post(const BoundaryArgs<S, Q>& b, const OpenArgs<S, Q>& o, cu
 // Fills natural-layout populations with the lattice weights (f = w).
 cudaError_t launch_fill_weights(double* obs_pop, long long ld, int n, int q, cudaStream_t st);
 
+// nw_mom holds float (narrow) or double values: the compute type of the
+// storage (FP32 for shifted storage, FP64 for FP64 storage).
 cudaError_t launch_nearwall_moments(int n_nw, const int* nw_node, const double* obs_mom, long long ld,
-                                    bool shifted, double* nw_mom, cudaStream_t st);
+                                    bool shifted, void* nw_mom, bool narrow, cudaStream_t st);
 
 // Reorders between the caller's [node][q] order and the engine's [q][ld] order;
 // perm[i] is the caller index of internal node i.

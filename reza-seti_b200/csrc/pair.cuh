@@ -62,12 +62,20 @@ constexpr int PAIR_THREADS = BLOCK_NODES / 2;
 // Resident CTAs per SM the phase-0 kernel is compiled for (caps registers).
 // Its loads carry no dependency, so occupancy is what keeps bytes in flight:
 // 6 CTAs (80 registers) for FP32, 8 (64 registers) for the 16-bit types,
-// whose 2-wide loads move half the bytes per instruction.
-template <class S>
+// whose 2-wide loads move half the bytes per instruction. D3Q27 holds 27
+// pairs of values and gets its own caps.
+template <class S, int Q>
 constexpr int pair0_min_blocks() {
 #ifdef LBM_PAIR0_MIN_BLOCKS
     return LBM_PAIR0_MIN_BLOCKS;
 #else
+    if (Q == 27) {
+#ifdef LBM_PAIR0_MIN_BLOCKS_Q27
+        return LBM_PAIR0_MIN_BLOCKS_Q27;
+#else
+        return sizeof(S) == 4 ? 4 : 5;
+#endif
+    }
     return sizeof(S) == 4 ? 6 : 8;
 #endif
 }
@@ -279,7 +287,7 @@ __device__ __forceinline__ void pair_scatter1_twin(const StepArgs<S, Q>& a, cons
 
 // Phase 0 (local slots only), one pair per thread.
 template <class S, int Q, int OBS>
-__global__ void __launch_bounds__(PAIR_THREADS, pair0_min_blocks<S>()) pair_phase0_kernel(StepArgs<S, Q> a) {
+__global__ void __launch_bounds__(PAIR_THREADS, pair0_min_blocks<S, Q>()) pair_phase0_kernel(StepArgs<S, Q> a) {
     using L = Lat<Q>;
     using MT = typename Meta<Q>::T;
     using IO = PairIO<S>;
@@ -324,11 +332,18 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Resident CTAs per SM the phase-1 kernel is compiled for (caps its
 // registers): 5 (96 registers, no spills for D3Q19) for FP32, 6 (80) for the
 // 16-bit types, measured best on the 21.4M-node vessel.
-template <class S>
+template <class S, int Q>
 constexpr int pair1_min_blocks() {
 #ifdef LBM_PAIR1_MIN_BLOCKS
     return LBM_PAIR1_MIN_BLOCKS;
 #else
+    if (Q == 27) {
+#ifdef LBM_PAIR1_MIN_BLOCKS_Q27
+        return LBM_PAIR1_MIN_BLOCKS_Q27;
+#else
+        return sizeof(S) == 4 ? 4 : 5;
+#endif
+    }
     return sizeof(S) == 4 ? 5 : 6;
 #endif
 }
@@ -342,7 +357,7 @@ __host__ __device__ __forceinline__ int pair_buffer_bytes(int seg_smem_bytes) {
 }
 
 template <class S, int Q, int OBS>
-__global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S>()) pair_phase1_kernel(StepArgs<S, Q> a, int n_tiles) {
+__global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_phase1_kernel(StepArgs<S, Q> a, int n_tiles) {
     using MT = typename Meta<Q>::T;
     extern __shared__ __align__(16) unsigned char pair_smem[];
     const int tid = threadIdx.x;

@@ -75,7 +75,7 @@ cudaError_t launch_step(const StepArgs<S, Q>& a, int phase, int bc, int obs, cud
     if constexpr (Store<S>::SHIFTED) {
         // physics mode, shifted storage: two nodes per thread, 32-bit slot
         // indices (lattices beyond 2^32 slots use step_kernel)
-        if (bc == BC_PHYSICS && (long long)Q * a.ld < (1LL << 32)))
+        if (bc == BC_PHYSICS && (long long)Q * a.ld < (1LL << 32))
             return phase ? pair_phase1<S, Q>(a, obs, st) : pair_phase0<S, Q>(a, obs, g, st);
     }
     if (bc == BC_REFERENCE) {

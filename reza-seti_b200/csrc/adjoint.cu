@@ -631,6 +631,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         const MT m0 = g.meta[n0];
         const MT m1 = live1 ? g.meta[n0 + 1] : MT(0);
         const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
+        // the node's own f^t does not depend on the neighbour rows: load it
+        // first, so that its latency overlaps the metadata -> row -> gather chain
+        float2 dpre[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) dpre[q] = *reinterpret_cast<const float2*>(D + (q * ld + u0));
         const int* sd0 = nbr_row<Q>(g.seg_base, g.seg_delta, n0, m0);
         float2 mu[Q];
         float gin0 = 0.f, gin1 = 0.f;
@@ -664,7 +669,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         float2 ra = f2s(0.f), rb = f2s(0.f), j0 = f2s(0.f), j1 = f2s(0.f), j2 = f2s(0.f), mud = f2s(0.f);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const float2 dq = *reinterpret_cast<const float2*>(D + (q * ld + u0));
+            const float2 dq = dpre[q];
             if (q & 1) rb = f2add(rb, dq);
             else ra = f2add(ra, dq);
             if (L::cx(q)) j0 = L::cx(q) > 0 ? f2add(j0, dq) : f2sub(j0, dq);

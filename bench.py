@@ -587,9 +587,12 @@ def run_voxel(torch, device):
     tris = G.tube_triangles(lambda z: (0.37, 0.21), lambda z: 16.0, 0.0, 128.0, 64, 32)
     ops = [G.opening("inlet", "z", 0.0, (0, 0, -1)), G.opening("outlet", "z", 128.0, (0, 0, 1))]
     G.voxelise_stl(tris, 0.5, ops, device=device)  # warm-up (context, module load)
-    t0 = time.perf_counter()
-    topo, (dims, origin, sp, ms) = G.voxelise_stl(tris, 0.5, ops, device=device, info=True)
-    wall = time.perf_counter() - t0
+    wall = None
+    for _ in range(3):  # best of three: the call is short, host jitter is not
+        t0 = time.perf_counter()
+        topo, (dims, origin, sp, ms) = G.voxelise_stl(tris, 0.5, ops, device=device, info=True)
+        dt = time.perf_counter() - t0
+        wall = dt if wall is None else min(wall, dt)
     pipe = {"triangles": len(tris), "grid_points": int(np.prod(dims)), "nodes": len(topo["kind"]),
             "near_wall_nodes": len(topo["nearwall"]), "gpu_seconds": round(wall, 4)}
     harness = os.path.join(ROOT, "oracle", "_ref", "refharness")

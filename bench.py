@@ -13,8 +13,10 @@ the geometry is analytic and the initial state is f = w). The population
 state (>= 1.6 GB) is larger than L2 (126 MB), so no flush is needed between
 steps.
 
-A step is one time step over every fluid node: the boundary pre-pass (WSS of
-near-wall nodes, outlet sources) and the AA stream+collide kernel. `value`
+A step is one time step over every fluid node: the AA stream+collide kernel
+and the post pass after it (that step's WSS on the near-wall nodes and the
+open-boundary corrections; in reference mode a pre-pass with the previous
+step's WSS and the outlet sources). `value`
 is fluid-node updates per second over all GPUs (MLUPS), timed with CUDA
 events on the engine's stream; `e2e` times the same through the C ABI from
 host buffers (state upload, steps, state and WSS download). With --gpus N

@@ -111,3 +111,16 @@ class PhysicsRef:
     def run(self, steps, scale=1.0):
         for _ in range(steps):
             self.step(scale)
+
+
+def womersley_shape(r, R, alpha):
+    """Complex axial-velocity shape of oscillatory pipe flow per unit flow-rate
+    amplitude (Womersley): u(r, t) = Re{Q e^{iwt} shape(r)}, with
+    shape = [1 - J0(b r/R) / J0(b)] / (pi R^2 [1 - 2 J1(b) / (b J0(b))]),
+    b = i^{3/2} alpha, alpha = R sqrt(w / nu). It integrates to 1 over the
+    cross-section and tends to the Poiseuille shape 2 (1 - r^2/R^2) / (pi R^2)
+    as alpha -> 0."""
+    from scipy.special import jv
+    b = alpha * np.exp(0.75j * np.pi)
+    j0 = jv(0, b)
+    return (1.0 - jv(0, b * np.asarray(r) / R) / j0) / (np.pi * R * R * (1.0 - 2.0 * jv(1, b) / (b * j0)))

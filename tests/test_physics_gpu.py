@@ -59,7 +59,8 @@ def test_harmonic_waveform_scales_inlet():
     assert rel(e.populations(), ref.f) < 1e-12
 
 
-def test_poiseuille_profile_and_mass_balance():
+@pytest.mark.parametrize("q", [19, 27])
+def test_poiseuille_profile_and_mass_balance(q):
     """Pipe R=8, tau 0.8 (nu = 0.1), parabolic inlet u_max = 0.02, outlet
     rho = 1, 6000 steps (six viscous times R^2/nu). The axial velocity at mid-
     length is the Hagen-Poiseuille parabola: a least-squares fit
@@ -69,7 +70,7 @@ def test_poiseuille_profile_and_mass_balance():
     0.5 %."""
     R, u_max = 8.0, 0.02
     topo = G.straight_pipe(radius=R, length=64)
-    e = physics_engine(topo, 0.8, u_max=u_max)
+    e = physics_engine(topo, 0.8, q=q, u_max=u_max)
     e.step(6000)
     rho, u = e.macros()
     c = topo["coords"]
@@ -98,7 +99,8 @@ def test_fp32_storage_tracks_fp64(q):
     assert rel(b.wss()[0], a.wss()[0]) < 1e-4
 
 
-def test_womersley_pulsatile_profile():
+@pytest.mark.parametrize("q", [19, 27])
+def test_womersley_pulsatile_profile(q):
     """Pipe R=8, tau 0.8 (nu = 0.1), inflow u_max 0.02 (1 + 0.8 cos wt) with a
     period of 251 steps: Womersley number alpha = R sqrt(w/nu) = 4. After
     6000 steps, the axial velocity at mid-length is sampled every step for one
@@ -116,7 +118,7 @@ def test_womersley_pulsatile_profile():
     w = alpha ** 2 * nu / R ** 2
     period = 2 * np.pi / w
     topo = G.straight_pipe(radius=R, length=64)
-    e = physics_engine(topo, 0.8, u_max=u_max)
+    e = physics_engine(topo, 0.8, q=q, u_max=u_max)
     e.set_waveform(period, [amp], [0.0])
     e.set_flow(False, 0.0, harmonic=True)
     e.set_observation(False)
@@ -145,7 +147,7 @@ def test_womersley_pulsatile_profile():
     qst = q1 * 2 * (1 - rr * rr / Re_ ** 2) / (np.pi * Re_ ** 2)
     err_w = np.linalg.norm(u1 - wom) / np.linalg.norm(wom)
     err_q = np.linalg.norm(u1 - qst) / np.linalg.norm(wom)
-    print("first harmonic: womersley rel L2 %.4f, quasi-steady %.4f, R_eff %.3f, |q1|/q0 %.3f"
-          % (err_w, err_q, Re_, abs(q1) / um.sum()))
+    print("D3Q%d first harmonic: womersley rel L2 %.4f, quasi-steady %.4f, R_eff %.3f, |q1|/q0 %.3f"
+          % (q, err_w, err_q, Re_, abs(q1) / um.sum()))
     assert err_w < 0.08
     assert err_q > 2 * err_w

@@ -624,19 +624,31 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                          double* __restrict__ domega) {
     using L = Lat<Q>;
     using MT = typename Meta<Q>::T;
+    extern __shared__ int pull_rows[];
     const int n0 = blockIdx.x * BLOCK_NODES + 2 * threadIdx.x;
-    double wl = 0.0;
-    if (n0 < g.n) {
-        const bool live1 = n0 + 1 < g.n;
-        const MT m0 = g.meta[n0];
-        const MT m1 = live1 ? g.meta[n0 + 1] : MT(0);
-        const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
-        // the node's own f^t does not depend on the neighbour rows: load it
-        // first, so that its latency overlaps the metadata -> row -> gather chain
-        float2 dpre[Q];
+    const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
+    const bool live0 = n0 < g.n;
+    // the node's own f^t and word do not depend on the neighbour rows: load
+    // them first, so that their latency overlaps the staging of the block's
+    // segment rows in shared memory (one barrier, as the engine's kernels do)
+    const MT m0 = live0 ? g.meta[n0] : MT(0);
+    const MT m1 = n0 + 1 < g.n ? g.meta[n0 + 1] : MT(0);
+    float2 dpre[Q];
+    if (live0) {
 #pragma unroll
         for (int q = 0; q < Q; ++q) dpre[q] = *reinterpret_cast<const float2*>(D + (q * ld + u0));
-        const int* sd0 = nbr_row<Q>(g.seg_base, g.seg_delta, n0, m0);
+    }
+    {
+        const int s0 = __ldg(g.seg_base + blockIdx.x);
+        const int cnt = (__ldg(g.seg_base + blockIdx.x + 1) - s0) * Q;
+        const int* src = g.seg_delta + (long long)s0 * Q;
+        for (int i = threadIdx.x; i < cnt; i += PAIR_THREADS) pull_rows[i] = __ldg(src + i);
+        __syncthreads();
+    }
+    double wl = 0.0;
+    if (live0) {
+        const bool live1 = n0 + 1 < g.n;
+        const int* sd0 = pull_rows + Q * (int)(m0 >> Meta<Q>::SEG_SHIFT);
         float2 mu[Q];
         float gin0 = 0.f, gin1 = 0.f;
         unsigned ol0 = 0, ol1 = 0;
@@ -656,7 +668,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
 #pragma unroll
             for (int q = 0; q < Q; ++q) mu[q].x = t[q];
             if (live1) {
-                pull_gather_node<Q>(g, Ln, n0 + 1, m1, nbr_row<Q>(g.seg_base, g.seg_delta, n0 + 1, m1), t, gin1,
+                pull_gather_node<Q>(g, Ln, n0 + 1, m1, pull_rows + Q * (int)(m1 >> Meta<Q>::SEG_SHIFT), t, gin1,
                                     ol1);
 #pragma unroll
                 for (int q = 0; q < Q; ++q) mu[q].y = t[q];
@@ -881,6 +893,16 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     // FP32 runs the node-pair kernels (32-bit slot indices)
     const bool pairs = std::is_same<R, float>::value && (long long)Q * s.ld < (1LL << 32);
     const dim3 pgrid((unsigned)((s.n + BLOCK_NODES - 1) / BLOCK_NODES));
+    // the pull kernel stages its block's segment rows in shared memory
+    const int pull_smem = s.max_block_segs * Q * (int)sizeof(int);
+    if (pairs && pull_smem > 48 * 1024) {
+        const cudaError_t ca = cudaFuncSetAttribute(adj_pull_pair_kernel<Q>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, pull_smem);
+        if (ca != cudaSuccess) {
+            o.err = std::string("adjoint pull kernel shared memory: ") + cudaGetErrorString(ca);
+            return -2;
+        }
+    }
     auto push = [&](const R* D, R* Dn, int64_t t) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
@@ -893,7 +915,8 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     auto pull = [&](const R* D, const R* Ln, R* Lc, int64_t t) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
-                adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, 0, st>>>(g, D, Ln, Lc, s.factors[t], dspeed, scal + N_PARTIALS);
+                adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, pull_smem, st>>>(g, D, Ln, Lc, s.factors[t], dspeed,
+                                                                                  scal + N_PARTIALS);
                 return;
             }
         }

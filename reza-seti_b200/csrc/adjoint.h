@@ -22,6 +22,7 @@ struct AdjointSetup {
     const void* meta = nullptr;      // Meta<Q>::T [n]
     const int* seg_base = nullptr;
     const int* seg_delta = nullptr;
+    int max_block_segs = 1;          // most segments of one BLOCK_NODES block (shared-memory rows)
     const int* aux = nullptr;        // inlet / outlet / near-wall table index per node
     double in_normal[3] = {0, 0, 0}; // outward inlet normal
     int n_in = 0;

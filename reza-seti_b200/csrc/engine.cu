@@ -1105,6 +1105,7 @@ int lbm_adjoint_run(lbm_engine* e, const lbm_adjoint_desc* d, int32_t gradient, 
     s.meta = e->meta;
     s.seg_base = e->seg_base;
     s.seg_delta = e->seg_delta;
+    s.max_block_segs = e->t.max_block_segs;
     s.aux = e->aux;
     for (int c = 0; c < 3; ++c) s.in_normal[c] = e->inlet_normal[c];
     s.n_in = n_in;

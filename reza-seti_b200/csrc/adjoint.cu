@@ -39,6 +39,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <cstdlib>
+#include <cstring>
 #include <type_traits>
 
 #include "adjoint.h"
@@ -453,6 +455,137 @@ __global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restric
         g -= A + B0 * c0 + B1 * c1 + B2 * c2;
     }
     if (on) Lc[(long long)q * a.ld + n] += (R)g;
+}
+
+// The same two objective kernels with one thread per target, for large
+// target sets: a thread keeps the target's Q values in registers and sums
+// them in direction order, where the warp forms spend most of their
+// instructions on FP64 shuffle reductions (sums here run in another order,
+// so results agree to rounding). Used when there are enough targets to fill
+// the GPU with threads.
+constexpr int OBJ_THREAD_MIN_TARGETS = 8192;
+
+template <class R, int Q>
+__global__ void __launch_bounds__(128) adj_objective_thread_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, int t) {
+    using L = Lat<Q>;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double jl = 0.0;
+    if (k < a.n_target) {
+        const int n = a.node[k];
+        R d[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d[q] = D[(long long)q * a.ld + n];
+        double drho = 0.0, j0 = 0.0, j1 = 0.0, j2 = 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double v = (double)d[q];
+            drho += v;
+            j0 += L::cx(q) * v;
+            j1 += L::cy(q) * v;
+            j2 += L::cz(q) * v;
+        }
+        const double rho = 1.0 + drho;
+        double* mt = a.mom + ((long long)t * a.n_target + k) * 4;
+        if (t >= 1) {
+            const double* mp = mt - 4 * (long long)a.n_target;
+            const R up[3] = {(R)mp[1], (R)mp[2], (R)mp[3]};
+            const double* nrm = a.nw_normal + 3 * (long long)a.nw[k];
+            double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const double c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+                const double cn = c0 * nrm[0] + c1 * nrm[1] + c2 * nrm[2];
+                const double f = (double)(d[q] - deq<R, Q>(q, (R)mp[0], up)) * cn;
+                t0 += f * (c0 - cn * nrm[0]);
+                t1 += f * (c1 - cn * nrm[1]);
+                t2 += f * (c2 - cn * nrm[2]);
+            }
+            t0 *= a.cw;
+            t1 *= a.cw;
+            t2 *= a.cw;
+            if (a.osi) {
+                double* ac = a.acc + 4 * (long long)k;
+                ac[0] += t0;
+                ac[1] += t1;
+                ac[2] += t2;
+                ac[3] += sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+            } else {
+                jl = a.inv_T * (t0 * t0 + t1 * t1 + t2 * t2);
+            }
+        }
+        mt[0] = drho;
+        mt[1] = j0 / rho;
+        mt[2] = j1 / rho;
+        mt[3] = j2 / rho;
+    }
+    warp_accumulate(jl, a.J);
+}
+
+template <class R, int Q>
+__global__ void __launch_bounds__(128)
+    adj_objective_adjoint_thread_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, const R* __restrict__ Dn,
+                                        R* __restrict__ Lc, int t, int T) {
+    using L = Lat<Q>;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n_target) return;
+    const int n = a.node[k];
+    const double* nrm = a.nw_normal + 3 * (long long)a.nw[k];
+    const double* coef = a.osi ? a.coef + 4 * (long long)k : nullptr;
+    // traction of populations src with the f_eq of moments m (drho, u)
+    auto traction = [&](const R* src, const double* m, double tau[3]) {
+        const R um[3] = {(R)m[1], (R)m[2], (R)m[3]};
+        tau[0] = tau[1] = tau[2] = 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+            const double cn = c0 * nrm[0] + c1 * nrm[1] + c2 * nrm[2];
+            const double f = (double)(src[(long long)q * a.ld + n] - deq<R, Q>(q, (R)m[0], um)) * cn;
+            tau[0] += f * (c0 - cn * nrm[0]);
+            tau[1] += f * (c1 - cn * nrm[1]);
+            tau[2] += f * (c2 - cn * nrm[2]);
+        }
+        for (int c = 0; c < 3; ++c) tau[c] *= a.cw;
+    };
+    // g_q = cw cn_q (dtp . m_q) - (A + B . c_q): dtp = dJ_t/dtau^t (t >= 1), and
+    // A, B the f_eq adjoint of dJ_{t+1}/dtau^{t+1} at the moments of f^t (t < T)
+    double dtp[3] = {0.0, 0.0, 0.0}, A = 0.0, B0 = 0.0, B1 = 0.0, B2 = 0.0;
+    if (t >= 1) {
+        const double* mp = a.mom + ((long long)(t - 1) * a.n_target + k) * 4;
+        double tau[3];
+        traction(D, mp, tau);
+        objective_dtau(a.osi, coef, a.inv_T, tau, dtp);
+    }
+    if (t < T) {
+        const double* mt = a.mom + ((long long)t * a.n_target + k) * 4;
+        double tau[3], dt[3];
+        traction(Dn, mt, tau);
+        objective_dtau(a.osi, coef, a.inv_T, tau, dt);
+        const double u[3] = {mt[1], mt[2], mt[3]};
+        const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+            const double cn = c0 * nrm[0] + c1 * nrm[1] + c2 * nrm[2];
+            const double gq =
+                a.cw * cn * (dt[0] * (c0 - cn * nrm[0]) + dt[1] * (c1 - cn * nrm[1]) + dt[2] * (c2 - cn * nrm[2]));
+            const double cu = c0 * u[0] + c1 * u[1] + c2 * u[2];
+            const double gw = gq * L::w(q);
+            const double kk = 3.0 + 9.0 * cu;
+            A += gw * (1.0 - 4.5 * cu * cu + 1.5 * usq);
+            B0 += gw * (kk * c0 - 3.0 * u[0]);
+            B1 += gw * (kk * c1 - 3.0 * u[1]);
+            B2 += gw * (kk * c2 - 3.0 * u[2]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+        const double cn = c0 * nrm[0] + c1 * nrm[1] + c2 * nrm[2];
+        const double g = a.cw * cn * (dtp[0] * (c0 - cn * nrm[0]) + dtp[1] * (c1 - cn * nrm[1]) +
+                                      dtp[2] * (c2 - cn * nrm[2])) -
+                         (A + B0 * c0 + B1 * c1 + B2 * c2);
+        Lc[(long long)q * a.ld + n] += (R)g;
+    }
 }
 
 // ------------------------------------------------ FP32 kernels, node pairs ---
@@ -890,6 +1023,14 @@ int run(const AdjointSetup& s, AdjointOut& o) {
 
     const dim3 grid((unsigned)((s.n + AT - 1) / AT));
     const unsigned tgrid = (unsigned)((nt + 3) / 4);  // one warp per target, 4 per block
+    // one thread per target once there are enough targets to fill the GPU;
+    // LBM_B200_OBJECTIVE_FORM=thread|warp picks a form (tests compare them)
+    bool obj_threads = nt >= OBJ_THREAD_MIN_TARGETS;
+    if (const char* form = getenv("LBM_B200_OBJECTIVE_FORM")) {
+        if (!strcmp(form, "thread")) obj_threads = true;
+        else if (!strcmp(form, "warp")) obj_threads = false;
+    }
+    const unsigned tgrid_t = (unsigned)((nt + 127) / 128);
     // FP32 runs the node-pair kernels (32-bit slot indices)
     const bool pairs = std::is_same<R, float>::value && (long long)Q * s.ld < (1LL << 32);
     const dim3 pgrid((unsigned)((s.n + BLOCK_NODES - 1) / BLOCK_NODES));
@@ -923,7 +1064,8 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         adj_pull_kernel<R, Q><<<grid, AT, 0, st>>>(g, D, Ln, Lc, s.factors[t], dspeed, scal + N_PARTIALS);
     };
     auto objective = [&](const R* D, int64_t t) {
-        if (nt) adj_objective_kernel<R, Q><<<tgrid, 128, 0, st>>>(oa, D, (int)t);
+        if (nt && obj_threads) adj_objective_thread_kernel<R, Q><<<tgrid_t, 128, 0, st>>>(oa, D, (int)t);
+        else if (nt) adj_objective_kernel<R, Q><<<tgrid, 128, 0, st>>>(oa, D, (int)t);
     };
     Events ev;
     cudaEventRecord(ev.e[0], st);
@@ -1008,7 +1150,10 @@ int run(const AdjointSetup& s, AdjointOut& o) {
                 } else {
                     pull(seg[t - t0], Lnext, Lcur, t);
                 }
-                if (nt)
+                if (nt && obj_threads)
+                    adj_objective_adjoint_thread_kernel<R, Q><<<tgrid_t, 128, 0, st>>>(
+                        oa, seg[t - t0], t < T ? seg[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
+                else if (nt)
                     adj_objective_adjoint_kernel<R, Q><<<tgrid, 128, 0, st>>>(
                         oa, seg[t - t0], t < T ? seg[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
                 std::swap(Lnext, Lcur);

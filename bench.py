@@ -817,7 +817,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    # warm-up of at least 200 steps before timing: the flow develops past the
+    # start-up transient and the clocks settle
+    ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="engine")
     ap.add_argument("--workload", default="tortuous8")
     ap.add_argument("--storage", default="f32")

@@ -61,3 +61,36 @@ def test_create_without_gpu_reports_no_device():
     with pytest.raises(capi.LbmError) as ei:
         Engine(topo, tau=0.8)
     assert ei.value.code == capi.LBM_ERR_NO_DEVICE
+
+
+STRUCTS = {"LbmDesc": "lbm_desc", "LbmAdjointDesc": "lbm_adjoint_desc", "LbmAdjointResult": "lbm_adjoint_result",
+           "LbmOpening": "lbm_opening", "LbmVoxelDesc": "lbm_voxel_desc", "LbmPulseDesc": "lbm_pulse_desc",
+           "LbmEquation": "lbm_equation", "LbmConfig": "lbm_config"}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every ctypes structure of the binding has the size and field offsets a C
+    compiler gives the header's typedef (a program built against
+    include/lbm_b200.h prints them)."""
+    import os
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lbm_b200.h"', "int main(void) {"]
+    want = []
+    for py, c in STRUCTS.items():
+        cls = getattr(capi, py)
+        lines.append('printf("%%zu\\n", sizeof(%s));' % c)
+        want.append(ctypes.sizeof(cls))
+        for name, _ in cls._fields_:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (c, name))
+            want.append(getattr(cls, name).offset)
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.dirname(capi.HEADER_PATH), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == want

@@ -270,10 +270,11 @@ __device__ __forceinline__ void objective_dtau(int osi, const double* coef, doub
 // target and one lane per direction: records the moments of f^t and adds
 // |tau^t|^2 / T for t >= 1.
 template <class R, int Q>
-__global__ void adj_objective_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, int t) {
+__device__ __forceinline__ void objective_warp_body(const ObjArgs<R, Q>& a, const R* __restrict__ D, int t,
+                                                    int bid) {
     using L = Lat<Q>;
     const int lane = threadIdx.x & 31;
-    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int k = bid * (blockDim.x >> 5) + (threadIdx.x >> 5);
     double jl = 0.0;
     if (k < a.n_target) {  // uniform over the warp
         const int n = a.node[k];
@@ -316,6 +317,11 @@ __global__ void adj_objective_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, i
         }
     }
     warp_accumulate(jl, a.J);
+}
+
+template <class R, int Q>
+__global__ void adj_objective_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, int t) {
+    objective_warp_body<R, Q>(a, D, t, blockIdx.x);
 }
 
 // lambda^t from lambda^{t+1} at every node (the transpose of the push). One
@@ -466,9 +472,10 @@ __global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restric
 constexpr int OBJ_THREAD_MIN_TARGETS = 8192;
 
 template <class R, int Q>
-__global__ void __launch_bounds__(128) adj_objective_thread_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, int t) {
+__device__ __forceinline__ void objective_thread_body(const ObjArgs<R, Q>& a, const R* __restrict__ D, int t,
+                                                      int bid) {
     using L = Lat<Q>;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = bid * blockDim.x + threadIdx.x;
     double jl = 0.0;
     if (k < a.n_target) {
         const int n = a.node[k];
@@ -519,6 +526,11 @@ __global__ void __launch_bounds__(128) adj_objective_thread_kernel(ObjArgs<R, Q>
         mt[3] = j2 / rho;
     }
     warp_accumulate(jl, a.J);
+}
+
+template <class R, int Q>
+__global__ void __launch_bounds__(128) adj_objective_thread_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, int t) {
+    objective_thread_body<R, Q>(a, D, t, blockIdx.x);
 }
 
 template <class R, int Q>
@@ -670,11 +682,11 @@ __device__ __forceinline__ void push_scatter_node(const AGeom<float, Q>& g, floa
 }
 
 template <int Q>
-__global__ void __launch_bounds__(PAIR_THREADS, 6)
-    adj_push_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t) {
+__device__ __forceinline__ void push_pair_body(const AGeom<float, Q>& g, const float* __restrict__ D,
+                                               float* __restrict__ Dn, double s_t, int bid) {
     using L = Lat<Q>;
     using MT = typename Meta<Q>::T;
-    const int n0 = blockIdx.x * BLOCK_NODES + 2 * threadIdx.x;
+    const int n0 = bid * BLOCK_NODES + 2 * threadIdx.x;
     if (n0 >= g.n) return;
     const bool live1 = n0 + 1 < g.n;
     const MT m0 = g.meta[n0];
@@ -709,6 +721,29 @@ __global__ void __launch_bounds__(PAIR_THREADS, 6)
             const float uy[3] = {u[0].y, u[1].y, u[2].y};
             push_scatter_node<Q>(g, Dn, n0 + 1, m1, nbr_row<Q>(g.seg_base, g.seg_delta, n0 + 1, m1), c, uy, s_t);
         }
+    }
+}
+
+template <int Q>
+__global__ void __launch_bounds__(PAIR_THREADS, 6)
+    adj_push_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t) {
+    push_pair_body<Q>(g, D, Dn, s_t, blockIdx.x);
+}
+
+// The forward sweep's objective term and push of one step in one launch: the
+// first obj_blocks blocks evaluate the objective at the targets, the others
+// push. Both read f^t; the objective writes only its per-target moments and
+// sums and the push only f^{t+1}, so the two run side by side instead of the
+// short objective launch idling the GPU before each push.
+template <int Q, bool THREADS>
+__global__ void __launch_bounds__(PAIR_THREADS, 6)
+    adj_push_objective_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t,
+                              ObjArgs<float, Q> a, int t, int obj_blocks) {
+    if ((int)blockIdx.x < obj_blocks) {
+        if (THREADS) objective_thread_body<float, Q>(a, D, t, blockIdx.x);
+        else objective_warp_body<float, Q>(a, D, t, blockIdx.x);
+    } else {
+        push_pair_body<Q>(g, D, Dn, s_t, (int)blockIdx.x - obj_blocks);
     }
 }
 
@@ -1067,14 +1102,32 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         if (nt && obj_threads) adj_objective_thread_kernel<R, Q><<<tgrid_t, 128, 0, st>>>(oa, D, (int)t);
         else if (nt) adj_objective_kernel<R, Q><<<tgrid, 128, 0, st>>>(oa, D, (int)t);
     };
+    // a forward step: objective term at f^t and the push to f^{t+1}, fused in
+    // one launch for the FP32 pair kernels
+    auto objective_push = [&](const R* D, R* Dn, int64_t t) {
+        if constexpr (std::is_same<R, float>::value) {
+            if (pairs && nt) {
+                const int ob = (int)(obj_threads ? tgrid_t : tgrid);
+                const dim3 fgrid(pgrid.x + (unsigned)ob);
+                if (obj_threads)
+                    adj_push_objective_kernel<Q, true><<<fgrid, PAIR_THREADS, 0, st>>>(g, D, Dn, s.factors[t], oa,
+                                                                                        (int)t, ob);
+                else
+                    adj_push_objective_kernel<Q, false><<<fgrid, PAIR_THREADS, 0, st>>>(g, D, Dn, s.factors[t], oa,
+                                                                                         (int)t, ob);
+                return;
+            }
+        }
+        objective(D, t);
+        push(D, Dn, t);
+    };
     Events ev;
     cudaEventRecord(ev.e[0], st);
     const R* fT = nullptr;
     if (!s.gradient) {
         adj_load_kernel<R, Q><<<grid, AT, 0, st>>>(s.f0, s.ld, s.n, seg[0]);
         for (int64_t t = 0; t < T; ++t) {
-            objective(seg[0], t);
-            push(seg[0], seg[1], t);
+            objective_push(seg[0], seg[1], t);
             std::swap(seg[0], seg[1]);
         }
         objective(seg[0], T);
@@ -1085,10 +1138,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         for (int64_t sg = 0; sg < nseg; ++sg) {
             const int64_t t0 = sg * K, t1 = std::min(T, t0 + K);
             seg[0] = ck[sg];
-            for (int64_t t = t0; t < t1; ++t) {
-                objective(seg[t - t0], t);
-                push(seg[t - t0], seg[t - t0 + 1], t);
-            }
+            for (int64_t t = t0; t < t1; ++t) objective_push(seg[t - t0], seg[t - t0 + 1], t);
             if (sg + 1 < nseg)
                 cudaMemcpyAsync(ck[sg + 1], seg[t1 - t0], field * sizeof(R), cudaMemcpyDeviceToDevice, st);
         }

@@ -963,6 +963,28 @@ struct Arena {
     }
 };
 
+// The reverse sweep's recomputation stream and the events that order it
+// against the main stream.
+struct AuxStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t forward_done = nullptr, reversed = nullptr, recomputed[2] = {nullptr, nullptr};
+    cudaError_t err = cudaSuccess;
+    cudaError_t init() {
+        err = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+        cudaEvent_t* evs[4] = {&forward_done, &reversed, &recomputed[0], &recomputed[1]};
+        for (cudaEvent_t* e : evs)
+            if (err == cudaSuccess) err = cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+        return err;
+    }
+    ~AuxStream() {
+        if (stream) cudaStreamSynchronize(stream);
+        cudaEvent_t evs[4] = {forward_done, reversed, recomputed[0], recomputed[1]};
+        for (cudaEvent_t e : evs)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
 struct Events {
     cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
     Events() {
@@ -988,6 +1010,10 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     // points at the segment's checkpoint
     std::vector<R*> seg((size_t)(s.gradient ? K + 1 : 2), nullptr);
     for (size_t j = s.gradient ? 1 : 0; j < seg.size(); ++j) seg[j] = ar.get<R>(field);
+    // a second set for the reverse sweep: the states of segment sg - 1 are
+    // recomputed into one set while segment sg's reverse steps read the other
+    std::vector<R*> seg2((size_t)(s.gradient && nseg > 1 ? K + 1 : 0), nullptr);
+    for (size_t j = 1; j < seg2.size(); ++j) seg2[j] = ar.get<R>(field);
     std::vector<R*> ck((size_t)(s.gradient ? nseg : 0));
     for (auto& p : ck) p = ar.get<R>(field);
     R* lam[2] = {nullptr, nullptr};
@@ -1079,15 +1105,16 @@ int run(const AdjointSetup& s, AdjointOut& o) {
             return -2;
         }
     }
-    auto push = [&](const R* D, R* Dn, int64_t t) {
+    auto push_on = [&](cudaStream_t stream, const R* D, R* Dn, int64_t t) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
-                adj_push_pair_kernel<Q><<<pgrid, PAIR_THREADS, 0, st>>>(g, D, Dn, s.factors[t]);
+                adj_push_pair_kernel<Q><<<pgrid, PAIR_THREADS, 0, stream>>>(g, D, Dn, s.factors[t]);
                 return;
             }
         }
-        adj_push_kernel<R, Q><<<grid, AT, 0, st>>>(g, D, Dn, s.factors[t]);
+        adj_push_kernel<R, Q><<<grid, AT, 0, stream>>>(g, D, Dn, s.factors[t]);
     };
+    auto push = [&](const R* D, R* Dn, int64_t t) { push_on(st, D, Dn, t); };
     auto pull = [&](const R* D, const R* Ln, R* Lc, int64_t t) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
@@ -1183,30 +1210,60 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         return -2;
     }
     if (s.gradient) {
-        // reverse sweep, segment by segment
+        // reverse sweep, segment by segment. The last segment's states are
+        // still in seg from the forward sweep; the states of segment sg - 1
+        // are recomputed on a second stream into the other set while the
+        // reverse steps of segment sg run, so the two overlap. The set a
+        // recomputation overwrites was last read by segment sg + 1's reverse
+        // steps, which it waits for.
         R* Lnext = lam[0];
         R* Lcur = lam[1];
+        std::vector<R*>* sets[2] = {&seg, &seg2};
+        AuxStream aux;
+        if (nseg > 1 && aux.init() != cudaSuccess) {
+            o.err = "adjoint recomputation stream: " + std::string(cudaGetErrorString(aux.err));
+            cudaStreamSynchronize(st);
+            return -2;
+        }
+        auto recompute = [&](int64_t sg) {
+            const int64_t t0 = sg * K, t1 = std::min(T, t0 + K);
+            std::vector<R*>& S = *sets[(nseg - 1 - sg) & 1];
+            S[0] = ck[sg];
+            for (int64_t t = t0; t < t1; ++t) push_on(aux.stream, S[t - t0], S[t - t0 + 1], t);
+            cudaEventRecord(aux.recomputed[sg & 1], aux.stream);
+            o.steps_recomputed += t1 - t0;
+        };
+        if (nseg > 1) {
+            // the checkpoints come from the forward sweep on st
+            cudaEventRecord(aux.forward_done, st);
+            cudaStreamWaitEvent(aux.stream, aux.forward_done, 0);
+            recompute(nseg - 2);
+        }
         for (int64_t sg = nseg - 1; sg >= 0; --sg) {
             const int64_t t0 = sg * K, t1 = std::min(T, t0 + K);
-            seg[0] = ck[sg];
-            if (sg + 1 < nseg) {
-                for (int64_t t = t0; t < t1; ++t) push(seg[t - t0], seg[t - t0 + 1], t);
-                o.steps_recomputed += t1 - t0;
-            }
+            std::vector<R*>& S = *sets[(nseg - 1 - sg) & 1];
+            S[0] = ck[sg];
+            if (sg + 1 < nseg) cudaStreamWaitEvent(st, aux.recomputed[sg & 1], 0);
             // lambda^{t1} of an earlier segment was finished by the later one
             for (int64_t t = (t1 == T ? T : t1 - 1); t >= t0; --t) {
                 if (t == T) {
                     cudaMemsetAsync(Lcur, 0, field * sizeof(R), st);
                 } else {
-                    pull(seg[t - t0], Lnext, Lcur, t);
+                    pull(S[t - t0], Lnext, Lcur, t);
                 }
                 if (nt && obj_threads)
                     adj_objective_adjoint_thread_kernel<R, Q><<<tgrid_t, 128, 0, st>>>(
-                        oa, seg[t - t0], t < T ? seg[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
+                        oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
                 else if (nt)
                     adj_objective_adjoint_kernel<R, Q><<<tgrid, 128, 0, st>>>(
-                        oa, seg[t - t0], t < T ? seg[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
+                        oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
                 std::swap(Lnext, Lcur);
+            }
+            if (sg >= 2) {
+                // segment sg - 2 goes into this segment's set once its reverse steps are done
+                cudaEventRecord(aux.reversed, st);
+                cudaStreamWaitEvent(aux.stream, aux.reversed, 0);
+                recompute(sg - 2);
             }
         }
         ce = cudaGetLastError();

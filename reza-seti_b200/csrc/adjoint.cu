@@ -66,6 +66,9 @@ struct AGeom {
     const float* out_nrm;   // [n_out][3]
     double out_rho;
     R omega;
+    // target index of each near-wall entry (-1: not a target), for the pull
+    // kernel that adds the objective's term to lambda at the targets
+    const int* nw_target;
 };
 
 template <int Q>
@@ -414,11 +417,12 @@ __global__ void __launch_bounds__(AT) adj_pull_kernel(AGeom<R, Q> g, const R* __
 // one lane per direction: dJ_t/df^t (t >= 1) and dJ_{t+1}/df^t through the
 // f_eq of tau^{t+1} (t < T).
 template <class R, int Q>
-__global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, const R* __restrict__ Dn,
-                                             R* __restrict__ Lc, int t, int T) {
+__device__ __forceinline__ void objective_adjoint_warp_body(const ObjArgs<R, Q>& a, const R* __restrict__ D,
+                                                            const R* __restrict__ Dn, R* __restrict__ Lc,
+                                                            R* __restrict__ Gout, int t, int T, int bid) {
     using L = Lat<Q>;
     const int lane = threadIdx.x & 31;
-    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int k = bid * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (k >= a.n_target) return;  // uniform over the warp
     const int n = a.node[k];
     const bool on = lane < Q;
@@ -460,7 +464,18 @@ __global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restric
         const double B2 = warp_sum(gw * (kk * c2 - 3.0 * u[2]));
         g -= A + B0 * c0 + B1 * c1 + B2 * c2;
     }
-    if (on) Lc[(long long)q * a.ld + n] += (R)g;
+    if (on) {
+        if (Gout) Gout[(long long)k * Q + q] = (R)g;
+        else Lc[(long long)q * a.ld + n] += (R)g;
+    }
+}
+
+// Adds the objective's term to lambda^t at the targets (Gout null), or
+// stores it per target in Gout[k][q] for the pull kernel to add.
+template <class R, int Q>
+__global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, const R* __restrict__ Dn,
+                                             R* __restrict__ Lc, int t, int T, R* __restrict__ Gout = nullptr) {
+    objective_adjoint_warp_body<R, Q>(a, D, Dn, Lc, Gout, t, T, blockIdx.x);
 }
 
 // The same two objective kernels with one thread per target, for large
@@ -785,15 +800,17 @@ __device__ __forceinline__ void pull_gather_node(const AGeom<float, Q>& g, const
     }
 }
 
+// Gadd (optional): the objective's term of this step per target, [target][Q],
+// added to lambda^t at the target nodes before it is stored.
 template <int Q>
-__global__ void __launch_bounds__(PAIR_THREADS, 4)
-    adj_pull_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
-                         float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
-                         double* __restrict__ domega) {
+__device__ __forceinline__ void pull_pair_body(const AGeom<float, Q>& g, const float* __restrict__ D,
+                                               const float* __restrict__ Ln, float* __restrict__ Lc, double s_t,
+                                               double* __restrict__ dspeed, double* __restrict__ domega,
+                                               const float* __restrict__ Gadd, int bid) {
     using L = Lat<Q>;
     using MT = typename Meta<Q>::T;
     extern __shared__ int pull_rows[];
-    const int n0 = blockIdx.x * BLOCK_NODES + 2 * threadIdx.x;
+    const int n0 = bid * BLOCK_NODES + 2 * threadIdx.x;
     const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
     const bool live0 = n0 < g.n;
     // the node's own f^t and word do not depend on the neighbour rows: load
@@ -807,8 +824,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         for (int q = 0; q < Q; ++q) dpre[q] = *reinterpret_cast<const float2*>(D + (q * ld + u0));
     }
     {
-        const int s0 = __ldg(g.seg_base + blockIdx.x);
-        const int cnt = (__ldg(g.seg_base + blockIdx.x + 1) - s0) * Q;
+        const int s0 = __ldg(g.seg_base + bid);
+        const int cnt = (__ldg(g.seg_base + bid + 1) - s0) * Q;
         const int* src = g.seg_delta + (long long)s0 * Q;
         for (int i = threadIdx.x; i < cnt; i += PAIR_THREADS) pull_rows[i] = __ldg(src + i);
         __syncthreads();
@@ -926,12 +943,21 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         // lambda_q = (1 - omega) mu_q + omega (A + B.c_q) + (G.c_q - G.u) / rho
         const float2 Ao = f2mul(om, A);
         const float2 ngu = f2mul(f2s(-1.f), f2mul(gu, irho));
+        // targets among the two nodes (near-wall nodes are plain fluid nodes,
+        // aux = their near-wall entry)
+        int tk0 = -1, tk1 = -1;
+        if (Gadd) {
+            if ((m0 >> Meta<Q>::NW_SHIFT) & 1) tk0 = g.nw_target[g.aux[n0]];
+            if (live1 && ((m1 >> Meta<Q>::NW_SHIFT) & 1)) tk1 = g.nw_target[g.aux[n0 + 1]];
+        }
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const float2 bc = cdot2<Q>(q, B);
             const float2 gc = cdot2<Q>(q, G);
             float2 lam = f2fma(keep, mu[q], f2fma(om, bc, Ao));
             lam = f2add(lam, f2fma(gc, irho, ngu));
+            if (tk0 >= 0) lam.x += Gadd[(long long)tk0 * Q + q];
+            if (tk1 >= 0) lam.y += Gadd[(long long)tk1 * Q + q];
             *reinterpret_cast<float2*>(Lc + (q * ld + u0)) = lam;
         }
         const float2 wq = f2sub(mueq, mud);
@@ -941,6 +967,32 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
             dspeed[g.aux[n0 + 1]] += (double)gin1 * s_t;
     }
     warp_accumulate(wl, domega);
+}
+
+template <int Q>
+__global__ void __launch_bounds__(PAIR_THREADS, 4)
+    adj_pull_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
+                         float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
+                         double* __restrict__ domega, const float* __restrict__ Gadd) {
+    pull_pair_body<Q>(g, D, Ln, Lc, s_t, dspeed, domega, Gadd, blockIdx.x);
+}
+
+// A reverse step with the next one's objective term in the same launch: the
+// first obj_blocks blocks compute the objective's term of step t - 1 into
+// Gnext (it needs f^{t-1} and f^t, not lambda), the others pull lambda^t and
+// add step t's term Gadd at the targets. The term then costs no launch of
+// its own and runs beside the pull.
+template <int Q>
+__global__ void __launch_bounds__(PAIR_THREADS, 4)
+    adj_pull_objective_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
+                              float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
+                              double* __restrict__ domega, const float* __restrict__ Gadd, ObjArgs<float, Q> a,
+                              const float* __restrict__ Dprev, float* __restrict__ Gnext, int t, int T,
+                              int obj_blocks) {
+    if ((int)blockIdx.x < obj_blocks)
+        objective_adjoint_warp_body<float, Q>(a, Dprev, D, nullptr, Gnext, t - 1, T, blockIdx.x);
+    else
+        pull_pair_body<Q>(g, D, Ln, Lc, s_t, dspeed, domega, Gadd, (int)blockIdx.x - obj_blocks);
 }
 
 struct Arena {
@@ -1029,12 +1081,17 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     double* scal = ar.get<double>(2 * N_PARTIALS);  // J, then dJ/domega partial sums
     int* tnode = ar.get<int>(std::max(nt, 1));
     int* tnw = ar.get<int>(std::max(nt, 1));
+    // objective term per target of two consecutive reverse steps, and the
+    // target index of each near-wall entry (FP32 pair kernels)
+    R* gterm[2] = {ar.get<R>((size_t)std::max(nt, 1) * Q), ar.get<R>((size_t)std::max(nt, 1) * Q)};
+    int* nw_target = ar.get<int>(std::max(s.n_nw, 1));
     if (ar.err != cudaSuccess) {
         o.err = std::string("adjoint buffers (") + std::to_string(ar.bytes >> 20) + " MiB allocated before): " +
                 cudaGetErrorString(ar.err);
         return -2;
     }
     o.bytes = ar.bytes;
+    bool unique_targets = true;  // a target listed twice keeps the per-step kernel
     {
         std::vector<int> tn(std::max(nt, 1)), tw(std::max(nt, 1));
         std::vector<int> nw_node(s.n_nw);
@@ -1045,6 +1102,12 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         }
         cudaMemcpyAsync(tnode, tn.data(), sizeof(int) * tn.size(), cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(tnw, tw.data(), sizeof(int) * tw.size(), cudaMemcpyHostToDevice, st);
+        std::vector<int> ntg((size_t)std::max(s.n_nw, 1), -1);
+        for (int k = 0; k < nt; ++k) {
+            if (ntg[s.targets[k]] >= 0) unique_targets = false;
+            ntg[s.targets[k]] = k;
+        }
+        cudaMemcpyAsync(nw_target, ntg.data(), sizeof(int) * ntg.size(), cudaMemcpyHostToDevice, st);
         if (s.n_in) cudaMemcpyAsync(speed, s.speed.data(), sizeof(double) * s.n_in, cudaMemcpyHostToDevice, st);
         cudaMemsetAsync(dspeed, 0, sizeof(double) * std::max(s.n_in, 1), st);
         cudaMemsetAsync(scal, 0, 2 * N_PARTIALS * sizeof(double), st);
@@ -1063,6 +1126,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     g.seg_base = s.seg_base;
     g.seg_delta = s.seg_delta;
     g.aux = s.aux;
+    g.nw_target = nw_target;
     for (int c = 0; c < 3; ++c) g.in_normal[c] = s.in_normal[c];
     g.speed = speed;
     g.out_nrm = s.out_nrm;
@@ -1119,7 +1183,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
                 adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, pull_smem, st>>>(g, D, Ln, Lc, s.factors[t], dspeed,
-                                                                                  scal + N_PARTIALS);
+                                                                                  scal + N_PARTIALS, nullptr);
                 return;
             }
         }
@@ -1245,18 +1309,42 @@ int run(const AdjointSetup& s, AdjointOut& o) {
             S[0] = ck[sg];
             if (sg + 1 < nseg) cudaStreamWaitEvent(st, aux.recomputed[sg & 1], 0);
             // lambda^{t1} of an earlier segment was finished by the later one
-            for (int64_t t = (t1 == T ? T : t1 - 1); t >= t0; --t) {
-                if (t == T) {
-                    cudaMemsetAsync(Lcur, 0, field * sizeof(R), st);
-                } else {
-                    pull(S[t - t0], Lnext, Lcur, t);
-                }
-                if (nt && obj_threads)
-                    adj_objective_adjoint_thread_kernel<R, Q><<<tgrid_t, 128, 0, st>>>(
-                        oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
-                else if (nt)
+            // FP32 pair kernels: the objective's term of each reverse step is
+            // computed one launch ahead into gterm (beside the previous pull)
+            // and added by the pull at the targets
+            bool staged = false;
+            // (target sets large enough for the thread form keep that form on
+            // its own: its warp-form term competes with the pull when fused)
+            if constexpr (std::is_same<R, float>::value) staged = pairs && nt > 0 && unique_targets && !obj_threads;
+            const int64_t top = t1 == T ? T : t1 - 1;
+            if constexpr (std::is_same<R, float>::value) {
+                const int64_t first_pull = t1 == T ? T - 1 : t1 - 1;
+                if (staged && first_pull >= t0)
                     adj_objective_adjoint_kernel<R, Q><<<tgrid, 128, 0, st>>>(
-                        oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
+                        oa, S[first_pull - t0], S[first_pull + 1 - t0], nullptr, (int)first_pull, (int)T,
+                        gterm[first_pull & 1]);
+            }
+            for (int64_t t = top; t >= t0; --t) {
+                if (t == T || !staged) {
+                    if (t == T) cudaMemsetAsync(Lcur, 0, field * sizeof(R), st);
+                    else pull(S[t - t0], Lnext, Lcur, t);
+                    if (nt && obj_threads)
+                        adj_objective_adjoint_thread_kernel<R, Q><<<tgrid_t, 128, 0, st>>>(
+                            oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
+                    else if (nt)
+                        adj_objective_adjoint_kernel<R, Q><<<tgrid, 128, 0, st>>>(
+                            oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
+                } else if constexpr (std::is_same<R, float>::value) {
+                    if (t - 1 >= t0) {
+                        const dim3 fgrid(pgrid.x + tgrid);
+                        adj_pull_objective_kernel<Q><<<fgrid, PAIR_THREADS, pull_smem, st>>>(
+                            g, S[t - t0], Lnext, Lcur, s.factors[t], dspeed, scal + N_PARTIALS, gterm[t & 1], oa,
+                            S[t - 1 - t0], gterm[(t - 1) & 1], (int)t, (int)T, (int)tgrid);
+                    } else {
+                        adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, pull_smem, st>>>(
+                            g, S[t - t0], Lnext, Lcur, s.factors[t], dspeed, scal + N_PARTIALS, gterm[t & 1]);
+                    }
+                }
                 std::swap(Lnext, Lcur);
             }
             if (sg >= 2) {

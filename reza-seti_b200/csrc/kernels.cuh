@@ -417,6 +417,10 @@ __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
     for (int q = 0; q < Q; ++q) s[q] = a.nw_s[(long long)q * a.n_nw + k];
     C* mom = a.nw_mom + 4 * (long long)k;
     const C* nd = a.nw_normal + 3 * (long long)k;
+    // the accumulators are read with the rest, not after the stores below:
+    // one memory round trip per node instead of two
+    double* acc = a.acc + 3 * (long long)k;
+    const double acc0 = acc[0], acc1 = acc[1], acc2 = acc[2], accm = a.accmag[k];
     double tau[3];
     if constexpr (sizeof(C) == 8) {
         // FP64: the reference's own triple loop, operand order kept
@@ -455,10 +459,10 @@ __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
     }
     const double w = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
     a.wss[k] = w;
-    a.acc[3 * (long long)k] += tau[0];
-    a.acc[3 * (long long)k + 1] += tau[1];
-    a.acc[3 * (long long)k + 2] += tau[2];
-    a.accmag[k] += w;
+    acc[0] = acc0 + tau[0];
+    acc[1] = acc1 + tau[1];
+    acc[2] = acc2 + tau[2];
+    a.accmag[k] = accm + w;
     // moments of these populations: the f_eq of the next step's WSS (the
     // same arithmetic as that step's collision of this node)
     C m0, u[3];

@@ -330,7 +330,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Resident CTAs per SM the phase-1 kernel is compiled for (caps its
-// registers): 5 (96 registers, no spills for D3Q19) for FP32, 6 (80) for the
+// registers): 5 (96 registers, no spills for D3Q19) for FP32, 7 (72) for the
 // 16-bit types, measured best on the 21.4M-node vessel.
 template <class S, int Q>
 constexpr int pair1_min_blocks() {
@@ -344,7 +344,7 @@ constexpr int pair1_min_blocks() {
         return sizeof(S) == 4 ? 4 : 5;
 #endif
     }
-    return sizeof(S) == 4 ? 5 : 6;
+    return sizeof(S) == 4 ? 5 : 7;
 #endif
 }
 

@@ -418,8 +418,8 @@ __global__ void __launch_bounds__(AT) adj_pull_kernel(AGeom<R, Q> g, const R* __
 // f_eq of tau^{t+1} (t < T).
 template <class R, int Q>
 __device__ __forceinline__ void objective_adjoint_warp_body(const ObjArgs<R, Q>& a, const R* __restrict__ D,
-                                                            const R* __restrict__ Dn, R* __restrict__ Lc,
-                                                            R* __restrict__ Gout, int t, int T, int bid) {
+                                                            const R* __restrict__ Dn, R* __restrict__ Lc, int t,
+                                                            int T, int bid) {
     using L = Lat<Q>;
     const int lane = threadIdx.x & 31;
     const int k = bid * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -464,18 +464,14 @@ __device__ __forceinline__ void objective_adjoint_warp_body(const ObjArgs<R, Q>&
         const double B2 = warp_sum(gw * (kk * c2 - 3.0 * u[2]));
         g -= A + B0 * c0 + B1 * c1 + B2 * c2;
     }
-    if (on) {
-        if (Gout) Gout[(long long)k * Q + q] = (R)g;
-        else Lc[(long long)q * a.ld + n] += (R)g;
-    }
+    if (on) Lc[(long long)q * a.ld + n] += (R)g;
 }
 
-// Adds the objective's term to lambda^t at the targets (Gout null), or
-// stores it per target in Gout[k][q] for the pull kernel to add.
+// Adds the objective's term to lambda^t at the targets.
 template <class R, int Q>
 __global__ void adj_objective_adjoint_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, const R* __restrict__ Dn,
-                                             R* __restrict__ Lc, int t, int T, R* __restrict__ Gout = nullptr) {
-    objective_adjoint_warp_body<R, Q>(a, D, Dn, Lc, Gout, t, T, blockIdx.x);
+                                             R* __restrict__ Lc, int t, int T) {
+    objective_adjoint_warp_body<R, Q>(a, D, Dn, Lc, t, T, blockIdx.x);
 }
 
 // The same two objective kernels with one thread per target, for large
@@ -548,13 +544,13 @@ __global__ void __launch_bounds__(128) adj_objective_thread_kernel(ObjArgs<R, Q>
     objective_thread_body<R, Q>(a, D, t, blockIdx.x);
 }
 
+// The objective's term of lambda^t at target k, one thread: added to Lc, or
+// stored in Gout[k][q] when Gout is given.
 template <class R, int Q>
-__global__ void __launch_bounds__(128)
-    adj_objective_adjoint_thread_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, const R* __restrict__ Dn,
-                                        R* __restrict__ Lc, int t, int T) {
+__device__ __forceinline__ void objective_adjoint_thread_body(const ObjArgs<R, Q>& a, const R* __restrict__ D,
+                                                              const R* __restrict__ Dn, R* __restrict__ Lc,
+                                                              R* __restrict__ Gout, int k, int t, int T) {
     using L = Lat<Q>;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a.n_target) return;
     const int n = a.node[k];
     const double* nrm = a.nw_normal + 3 * (long long)a.nw[k];
     const double* coef = a.osi ? a.coef + 4 * (long long)k : nullptr;
@@ -611,8 +607,38 @@ __global__ void __launch_bounds__(128)
         const double g = a.cw * cn * (dtp[0] * (c0 - cn * nrm[0]) + dtp[1] * (c1 - cn * nrm[1]) +
                                       dtp[2] * (c2 - cn * nrm[2])) -
                          (A + B0 * c0 + B1 * c1 + B2 * c2);
-        Lc[(long long)q * a.ld + n] += (R)g;
+        if (Gout) Gout[(long long)k * Q + q] = (R)g;
+        else Lc[(long long)q * a.ld + n] += (R)g;
     }
+}
+
+template <class R, int Q>
+__global__ void __launch_bounds__(128)
+    adj_objective_adjoint_thread_kernel(ObjArgs<R, Q> a, const R* __restrict__ D, const R* __restrict__ Dn,
+                                        R* __restrict__ Lc, int t, int T) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < a.n_target) objective_adjoint_thread_body<R, Q>(a, D, Dn, Lc, nullptr, k, t, T);
+}
+
+// The objective's terms of a whole checkpoint segment, steps t0 .. t0 +
+// n_steps - 1 (all below T), one thread per (step, target): a term needs
+// f^t, f^{t+1} and the forward sweep's moments, not lambda, so the segment's
+// terms are computed as soon as its states are, in one launch wide enough to
+// fill the GPU. State j of the segment is `first` for j = 0, else states[j];
+// the term of step t0 + j goes to Gout[j][k][q], which the pull of that step
+// adds at the targets.
+template <class R, int Q>
+__global__ void __launch_bounds__(128)
+    adj_objective_adjoint_segment_kernel(ObjArgs<R, Q> a, const R* const* __restrict__ states,
+                                         const R* __restrict__ first, int t0, int n_steps, int T,
+                                         R* __restrict__ Gout) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)n_steps * a.n_target) return;
+    const int j = (int)(i / a.n_target);
+    const int k = (int)(i - (long long)j * a.n_target);
+    const R* D = j == 0 ? first : states[j];
+    objective_adjoint_thread_body<R, Q>(a, D, states[j + 1], nullptr, Gout + (long long)j * a.n_target * Q, k,
+                                        t0 + j, T);
 }
 
 // ------------------------------------------------ FP32 kernels, node pairs ---
@@ -977,24 +1003,6 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     pull_pair_body<Q>(g, D, Ln, Lc, s_t, dspeed, domega, Gadd, blockIdx.x);
 }
 
-// A reverse step with the next one's objective term in the same launch: the
-// first obj_blocks blocks compute the objective's term of step t - 1 into
-// Gnext (it needs f^{t-1} and f^t, not lambda), the others pull lambda^t and
-// add step t's term Gadd at the targets. The term then costs no launch of
-// its own and runs beside the pull.
-template <int Q>
-__global__ void __launch_bounds__(PAIR_THREADS, 4)
-    adj_pull_objective_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
-                              float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
-                              double* __restrict__ domega, const float* __restrict__ Gadd, ObjArgs<float, Q> a,
-                              const float* __restrict__ Dprev, float* __restrict__ Gnext, int t, int T,
-                              int obj_blocks) {
-    if ((int)blockIdx.x < obj_blocks)
-        objective_adjoint_warp_body<float, Q>(a, Dprev, D, nullptr, Gnext, t - 1, T, blockIdx.x);
-    else
-        pull_pair_body<Q>(g, D, Ln, Lc, s_t, dspeed, domega, Gadd, (int)blockIdx.x - obj_blocks);
-}
-
 struct Arena {
     std::vector<void*> ptrs;
     size_t bytes = 0;
@@ -1081,9 +1089,31 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     double* scal = ar.get<double>(2 * N_PARTIALS);  // J, then dJ/domega partial sums
     int* tnode = ar.get<int>(std::max(nt, 1));
     int* tnw = ar.get<int>(std::max(nt, 1));
-    // objective term per target of two consecutive reverse steps, and the
-    // target index of each near-wall entry (FP32 pair kernels)
-    R* gterm[2] = {ar.get<R>((size_t)std::max(nt, 1) * Q), ar.get<R>((size_t)std::max(nt, 1) * Q)};
+    // FP32 pair kernels: the pull adds the objective's term of its step at
+    // the targets, a checkpoint segment's terms computed in one launch once
+    // its states are ready ("segment" staging). One target listed twice keeps
+    // a kernel per step that adds each entry ("step" staging, the only form
+    // of the FP64 kernels); LBM_B200_OBJECTIVE_STAGING=step|segment forces
+    // one (tests compare them).
+    bool unique_targets = true;
+    {
+        std::vector<char> seen((size_t)std::max(s.n_nw, 1), 0);
+        for (int k = 0; k < nt; ++k) {
+            if (seen[s.targets[k]]) unique_targets = false;
+            seen[s.targets[k]] = 1;
+        }
+    }
+    const bool pairs = std::is_same<R, float>::value && (long long)Q * s.ld < (1LL << 32);
+    bool seg_terms = pairs && s.gradient && nt > 0 && unique_targets;
+    if (const char* f = getenv("LBM_B200_OBJECTIVE_STAGING"); f && !strcmp(f, "step")) seg_terms = false;
+    // objective term per target of every step of a segment, one buffer per
+    // segment set: [step in segment][target][Q]
+    const size_t gsize = seg_terms ? (size_t)nt * Q * (size_t)K : 1;
+    R* gterm[2] = {ar.get<R>(gsize), ar.get<R>(gsize)};
+    // device copies of the two segment sets' state pointers (entry 0, the
+    // checkpoint, is passed on its own)
+    R** states_dev[2] = {ar.get<R*>((size_t)K + 1), ar.get<R*>((size_t)K + 1)};
+    // target index of each near-wall entry
     int* nw_target = ar.get<int>(std::max(s.n_nw, 1));
     if (ar.err != cudaSuccess) {
         o.err = std::string("adjoint buffers (") + std::to_string(ar.bytes >> 20) + " MiB allocated before): " +
@@ -1091,7 +1121,6 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         return -2;
     }
     o.bytes = ar.bytes;
-    bool unique_targets = true;  // a target listed twice keeps the per-step kernel
     {
         std::vector<int> tn(std::max(nt, 1)), tw(std::max(nt, 1));
         std::vector<int> nw_node(s.n_nw);
@@ -1103,10 +1132,11 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         cudaMemcpyAsync(tnode, tn.data(), sizeof(int) * tn.size(), cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(tnw, tw.data(), sizeof(int) * tw.size(), cudaMemcpyHostToDevice, st);
         std::vector<int> ntg((size_t)std::max(s.n_nw, 1), -1);
-        for (int k = 0; k < nt; ++k) {
-            if (ntg[s.targets[k]] >= 0) unique_targets = false;
-            ntg[s.targets[k]] = k;
-        }
+        for (int k = 0; k < nt; ++k) ntg[s.targets[k]] = k;
+        std::vector<R*> tab[2] = {seg, seg2.empty() ? seg : seg2};
+        for (auto& v : tab) v.resize((size_t)K + 1, nullptr);
+        for (int j = 0; j < 2; ++j)
+            cudaMemcpyAsync(states_dev[j], tab[j].data(), sizeof(R*) * ((size_t)K + 1), cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(nw_target, ntg.data(), sizeof(int) * ntg.size(), cudaMemcpyHostToDevice, st);
         if (s.n_in) cudaMemcpyAsync(speed, s.speed.data(), sizeof(double) * s.n_in, cudaMemcpyHostToDevice, st);
         cudaMemsetAsync(dspeed, 0, sizeof(double) * std::max(s.n_in, 1), st);
@@ -1156,8 +1186,6 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         else if (!strcmp(form, "warp")) obj_threads = false;
     }
     const unsigned tgrid_t = (unsigned)((nt + 127) / 128);
-    // FP32 runs the node-pair kernels (32-bit slot indices)
-    const bool pairs = std::is_same<R, float>::value && (long long)Q * s.ld < (1LL << 32);
     const dim3 pgrid((unsigned)((s.n + BLOCK_NODES - 1) / BLOCK_NODES));
     // the pull kernel stages its block's segment rows in shared memory
     const int pull_smem = s.max_block_segs * Q * (int)sizeof(int);
@@ -1179,11 +1207,11 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         adj_push_kernel<R, Q><<<grid, AT, 0, stream>>>(g, D, Dn, s.factors[t]);
     };
     auto push = [&](const R* D, R* Dn, int64_t t) { push_on(st, D, Dn, t); };
-    auto pull = [&](const R* D, const R* Ln, R* Lc, int64_t t) {
+    auto pull = [&](const R* D, const R* Ln, R* Lc, int64_t t, const R* Gadd) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
                 adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, pull_smem, st>>>(g, D, Ln, Lc, s.factors[t], dspeed,
-                                                                                  scal + N_PARTIALS, nullptr);
+                                                                                  scal + N_PARTIALS, Gadd);
                 return;
             }
         }
@@ -1289,14 +1317,26 @@ int run(const AdjointSetup& s, AdjointOut& o) {
             cudaStreamSynchronize(st);
             return -2;
         }
+        // the objective's terms of segment sg, once its states are in its
+        // set, into that set's term buffer
+        auto segment_terms = [&](cudaStream_t stream, int64_t sg) {
+            if (!seg_terms) return;
+            const int64_t t0 = sg * K, n_steps = std::min(T, t0 + K) - t0;
+            const int set = (int)((nseg - 1 - sg) & 1);
+            const unsigned blocks = (unsigned)((n_steps * nt + 127) / 128);
+            adj_objective_adjoint_segment_kernel<R, Q><<<blocks, 128, 0, stream>>>(
+                oa, states_dev[set], ck[sg], (int)t0, (int)n_steps, (int)T, gterm[set]);
+        };
         auto recompute = [&](int64_t sg) {
             const int64_t t0 = sg * K, t1 = std::min(T, t0 + K);
             std::vector<R*>& S = *sets[(nseg - 1 - sg) & 1];
             S[0] = ck[sg];
             for (int64_t t = t0; t < t1; ++t) push_on(aux.stream, S[t - t0], S[t - t0 + 1], t);
+            segment_terms(aux.stream, sg);
             cudaEventRecord(aux.recomputed[sg & 1], aux.stream);
             o.steps_recomputed += t1 - t0;
         };
+        segment_terms(st, nseg - 1);
         if (nseg > 1) {
             // the checkpoints come from the forward sweep on st
             cudaEventRecord(aux.forward_done, st);
@@ -1309,41 +1349,20 @@ int run(const AdjointSetup& s, AdjointOut& o) {
             S[0] = ck[sg];
             if (sg + 1 < nseg) cudaStreamWaitEvent(st, aux.recomputed[sg & 1], 0);
             // lambda^{t1} of an earlier segment was finished by the later one
-            // FP32 pair kernels: the objective's term of each reverse step is
-            // computed one launch ahead into gterm (beside the previous pull)
-            // and added by the pull at the targets
-            bool staged = false;
-            // (target sets large enough for the thread form keep that form on
-            // its own: its warp-form term competes with the pull when fused)
-            if constexpr (std::is_same<R, float>::value) staged = pairs && nt > 0 && unique_targets && !obj_threads;
+            const R* gseg = gterm[(nseg - 1 - sg) & 1];
             const int64_t top = t1 == T ? T : t1 - 1;
-            if constexpr (std::is_same<R, float>::value) {
-                const int64_t first_pull = t1 == T ? T - 1 : t1 - 1;
-                if (staged && first_pull >= t0)
-                    adj_objective_adjoint_kernel<R, Q><<<tgrid, 128, 0, st>>>(
-                        oa, S[first_pull - t0], S[first_pull + 1 - t0], nullptr, (int)first_pull, (int)T,
-                        gterm[first_pull & 1]);
-            }
             for (int64_t t = top; t >= t0; --t) {
-                if (t == T || !staged) {
+                if (t < T && seg_terms) {
+                    pull(S[t - t0], Lnext, Lcur, t, gseg + (size_t)(t - t0) * nt * Q);
+                } else {
                     if (t == T) cudaMemsetAsync(Lcur, 0, field * sizeof(R), st);
-                    else pull(S[t - t0], Lnext, Lcur, t);
+                    else pull(S[t - t0], Lnext, Lcur, t, nullptr);
                     if (nt && obj_threads)
                         adj_objective_adjoint_thread_kernel<R, Q><<<tgrid_t, 128, 0, st>>>(
                             oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
                     else if (nt)
                         adj_objective_adjoint_kernel<R, Q><<<tgrid, 128, 0, st>>>(
                             oa, S[t - t0], t < T ? S[t - t0 + 1] : nullptr, Lcur, (int)t, (int)T);
-                } else if constexpr (std::is_same<R, float>::value) {
-                    if (t - 1 >= t0) {
-                        const dim3 fgrid(pgrid.x + tgrid);
-                        adj_pull_objective_kernel<Q><<<fgrid, PAIR_THREADS, pull_smem, st>>>(
-                            g, S[t - t0], Lnext, Lcur, s.factors[t], dspeed, scal + N_PARTIALS, gterm[t & 1], oa,
-                            S[t - 1 - t0], gterm[(t - 1) & 1], (int)t, (int)T, (int)tgrid);
-                    } else {
-                        adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, pull_smem, st>>>(
-                            g, S[t - t0], Lnext, Lcur, s.factors[t], dspeed, scal + N_PARTIALS, gterm[t & 1]);
-                    }
                 }
                 std::swap(Lnext, Lcur);
             }

@@ -232,3 +232,28 @@ def test_objective_kernel_forms_agree(q, objective, monkeypatch):
     # FP32 adjoint states: the two sum orders differ at FP32 rounding (1.3e-5
     # measured), well inside the 1e-3 bound of FP32 against FP64
     assert rel(t["f32"]["grad_coeffs"], w["f32"]["grad_coeffs"]) < 1e-4
+
+
+@pytest.mark.parametrize("objective", ["wss2", "osi"])
+def test_objective_staging_forms_agree(objective, monkeypatch):
+    """FP32 pull kernels add each reverse step's objective term at the
+    targets, a checkpoint segment's terms computed in one launch (default)
+    instead of by a kernel per step (LBM_B200_OBJECTIVE_STAGING=step). With
+    the thread form of the term both do the same FP32 additions. Four
+    segments, the last one short, cover both segment sets."""
+    topo = stenosed_pipe()
+    basis = G.zernike_inlet_basis(topo, 8)
+    a = coefficients()
+    targets = G.stenotic_throat_targets(topo, 4.0)
+    e = Engine(topo, tau=0.6, storage="f64", bc="physics")
+    e.set_waveform(60.0, [1.5], [0.0])
+    e.set_flow(False, 0.0, harmonic=True)
+    monkeypatch.setenv("LBM_B200_OBJECTIVE_FORM", "thread")
+    out = {}
+    for staging in ("segment", "step"):
+        monkeypatch.setenv("LBM_B200_OBJECTIVE_STAGING", staging)
+        out[staging] = e.adjoint(130, targets, basis, a, checkpoint_every=40, precision="f32", objective=objective)
+    sg, st = out["segment"], out["step"]
+    assert sg["J"] == st["J"]
+    assert rel(sg["grad_coeffs"], st["grad_coeffs"]) < 1e-6
+    assert abs(sg["dJ_dtau"] - st["dJ_dtau"]) <= 1e-6 * abs(st["dJ_dtau"])

@@ -52,6 +52,16 @@ namespace {
 
 constexpr int AT = 256;  // threads per block of the node kernels
 
+// Resident CTAs per SM the FP32 pair kernels are compiled for (caps their
+// registers): push 6 (80 registers), pull 5 (96 registers, a few spilled:
+// faster than 4 at 128 registers, while 6 spills heavily).
+#ifndef LBM_ADJ_PUSH_MIN_BLOCKS
+#define LBM_ADJ_PUSH_MIN_BLOCKS 6
+#endif
+#ifndef LBM_ADJ_PULL_MIN_BLOCKS
+#define LBM_ADJ_PULL_MIN_BLOCKS 5
+#endif
+
 template <class R, int Q>
 struct AGeom {
     using MT = typename Meta<Q>::T;
@@ -766,7 +776,7 @@ __device__ __forceinline__ void push_pair_body(const AGeom<float, Q>& g, const f
 }
 
 template <int Q>
-__global__ void __launch_bounds__(PAIR_THREADS, 6)
+__global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
     adj_push_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t) {
     push_pair_body<Q>(g, D, Dn, s_t, blockIdx.x);
 }
@@ -777,7 +787,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 6)
 // sums and the push only f^{t+1}, so the two run side by side instead of the
 // short objective launch idling the GPU before each push.
 template <int Q, bool THREADS>
-__global__ void __launch_bounds__(PAIR_THREADS, 6)
+__global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
     adj_push_objective_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t,
                               ObjArgs<float, Q> a, int t, int obj_blocks) {
     if ((int)blockIdx.x < obj_blocks) {
@@ -996,7 +1006,7 @@ __device__ __forceinline__ void pull_pair_body(const AGeom<float, Q>& g, const f
 }
 
 template <int Q>
-__global__ void __launch_bounds__(PAIR_THREADS, 4)
+__global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PULL_MIN_BLOCKS)
     adj_pull_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
                          float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
                          double* __restrict__ domega, const float* __restrict__ Gadd) {

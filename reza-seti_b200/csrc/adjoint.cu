@@ -738,10 +738,13 @@ __device__ __forceinline__ void push_pair_body(const AGeom<float, Q>& g, const f
     using L = Lat<Q>;
     using MT = typename Meta<Q>::T;
     const int n0 = bid * BLOCK_NODES + 2 * threadIdx.x;
-    if (n0 >= g.n) return;
-    const bool live1 = n0 + 1 < g.n;
-    const MT m0 = g.meta[n0];
+    const bool live0 = n0 < g.n, live1 = n0 + 1 < g.n;
+    const MT m0 = live0 ? g.meta[n0] : MT(0);
     const MT m1 = live1 ? g.meta[n0 + 1] : MT(0);
+    // a warp whose every pair is a twin takes the twin path; mixed warps take
+    // the general one, which serves twins too, instead of running both
+    const bool twin = __all_sync(0xffffffffu, !live0 || adj_twin<Q>(m0, m1));
+    if (!live0) return;
     const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
     float2 s[Q];
 #pragma unroll
@@ -749,7 +752,7 @@ __device__ __forceinline__ void push_pair_body(const AGeom<float, Q>& g, const f
     float2 drho, u[3];
     collide_pair<Q>(s, g.omega, drho, u);
     const int* sd0 = nbr_row<Q>(g.seg_base, g.seg_delta, n0, m0);
-    if (adj_twin<Q>(m0, m1)) {
+    if (twin) {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             if (q == L::REST) {
@@ -867,13 +870,15 @@ __device__ __forceinline__ void pull_pair_body(const AGeom<float, Q>& g, const f
         __syncthreads();
     }
     double wl = 0.0;
+    const bool live1 = n0 + 1 < g.n;
+    // warp-uniform twin path, as in the push
+    const bool twin = __all_sync(0xffffffffu, !live0 || adj_twin<Q>(m0, m1));
     if (live0) {
-        const bool live1 = n0 + 1 < g.n;
         const int* sd0 = pull_rows + Q * (int)(m0 >> Meta<Q>::SEG_SHIFT);
         float2 mu[Q];
         float gin0 = 0.f, gin1 = 0.f;
         unsigned ol0 = 0, ol1 = 0;
-        if (adj_twin<Q>(m0, m1)) {
+        if (twin) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 if (q == L::REST) {

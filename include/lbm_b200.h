@@ -229,7 +229,8 @@ int lbm_get_info(lbm_engine* e, int64_t* n_nodes, int64_t* ld, int64_t* n_segmen
  * the definition and scale of lbm_get_wss. With gradient = 1 it also returns
  * dJ/dcoeffs, dJ/dtau and dJ/dv_i from a hand-written discrete adjoint: the
  * state is checkpointed every checkpoint_every steps, and the reverse sweep
- * recomputes each segment from its checkpoint (memory ~ (T/K + K) states). */
+ * recomputes each segment from its checkpoint, overlapped with the reverse
+ * steps of the later segment (memory ~ (T/K + 2K) states). */
 /* Objectives of lbm_adjoint_run. LBM_ADJOINT_OSI is the mean over the
  * targets of OSI_k = (1 - |A_k| / M_k) / 2 with A_k = sum_t tau_k^t and
  * M_k = sum_t |tau_k^t| (the accumulators of lbm_get_wss, taken over the

@@ -1105,21 +1105,13 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     int* tnode = ar.get<int>(std::max(nt, 1));
     int* tnw = ar.get<int>(std::max(nt, 1));
     // FP32 pair kernels: the pull adds the objective's term of its step at
-    // the targets, a checkpoint segment's terms computed in one launch once
-    // its states are ready ("segment" staging). One target listed twice keeps
-    // a kernel per step that adds each entry ("step" staging, the only form
-    // of the FP64 kernels); LBM_B200_OBJECTIVE_STAGING=step|segment forces
-    // one (tests compare them).
-    bool unique_targets = true;
-    {
-        std::vector<char> seen((size_t)std::max(s.n_nw, 1), 0);
-        for (int k = 0; k < nt; ++k) {
-            if (seen[s.targets[k]]) unique_targets = false;
-            seen[s.targets[k]] = 1;
-        }
-    }
+    // the targets (distinct, checked by adjoint_run), a checkpoint segment's
+    // terms computed in one launch once its states are ready ("segment"
+    // staging). The FP64 kernels keep a kernel per step that adds the term to
+    // lambda ("step" staging); LBM_B200_OBJECTIVE_STAGING=step forces it for
+    // FP32 too (tests compare the two).
     const bool pairs = std::is_same<R, float>::value && (long long)Q * s.ld < (1LL << 32);
-    bool seg_terms = pairs && s.gradient && nt > 0 && unique_targets;
+    bool seg_terms = pairs && s.gradient && nt > 0;
     if (const char* f = getenv("LBM_B200_OBJECTIVE_STAGING"); f && !strcmp(f, "step")) seg_terms = false;
     // objective term per target of every step of a segment, one buffer per
     // segment set: [step in segment][target][Q]

@@ -100,17 +100,26 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic_per_node(storage):
-    """DRAM bytes per fluid node and launch of the step kernel, from the
-    committed ncu summary (profiles/step_kernel_d3q19.md), or None."""
-    path = os.path.join(ROOT, "profiles", "step_kernel_d3q19.md")
+# DRAM bytes (read + write) per fluid node and step-kernel launch, averaged
+# over the two phase kernels of one step, from an ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum on the step kernels (command
+# and case in profiles/step_kernel_traffic_d3q19.md); None where not captured.
+STEP_KERNEL_TRAFFIC = {}
+TRAFFIC_SOURCE = None
+
+
+def host_cpu():
+    """CPU model and logical core count of this host (for the CPU baselines)."""
+    model = None
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_node_%s:" % storage):
-                return float(line.split(":")[1])
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
     except OSError:
         pass
-    return None
+    return {"cpu_model": model, "nproc": os.cpu_count()}
 
 
 class ClockSampler:
@@ -204,7 +213,10 @@ def replica_mlups(n_nodes, steps, max_ms, world):
 
 def time_engine(topo, storage, steps, warmup, device, torch, vel, bc="physics", radius=None, before=None):
     from lbm_b200 import Engine
-    eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device, bc=bc)
+    # reference boundaries diverge at tau 0.52 (as the reference itself does);
+    # their timing runs on through the non-finite values, as the reference would
+    eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device, bc=bc,
+                 numeric_check=(bc == "physics"))
     eng.set_flow(False, vel)
     if bc == "physics":
         eng.set_inlet_profile(inlet_profile(topo, radius, vel))
@@ -262,10 +274,11 @@ def run_gpu(args):
     alg_bytes = 2 * Q * S * n
     step_avg_ms = ms_step / args.steps
     achieved = alg_bytes / (step_avg_ms / 1e3) / 1e9
-    tpn = profile_traffic_per_node(storage)
+    tpn = STEP_KERNEL_TRAFFIC.get(storage)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": round(tpn * n) if tpn else None,
+                "traffic_source": TRAFFIC_SOURCE if tpn else "not captured for this storage type",
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "step_kernel_ms": round(step_avg_ms, 5),
                 "boundary_kernel_ms": round(ms_bnd / args.steps, 5)}
@@ -316,9 +329,61 @@ def run_gpu(args):
             "gpu_launches": 2 * args.steps, "clocks": clocks, "device_flags": flags,
             "variants": variants, "precision": precision, "adjoint": adjoint, "configs": configs, "geometry_setup": voxel,
         }
+        # the key figures once more, last on the line (a reader of its tail
+        # sees them)
+        line["summary"] = summary(storage, mlups, roofline, variants, precision, adjoint, configs, cpu)
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def summary(storage, mlups, roofline, variants, precision, adjoint, configs, cpu):
+    """Headline figures of every section, in one small block."""
+    def get(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    out = {storage + "_MLUPS": round(mlups, 1), "step_kernel_frac": roofline["frac"]}
+    for st in ("f32", "f16", "bf16"):
+        v = get(variants, st, "MLUPS")
+        if v is not None:
+            out[st + "_MLUPS"] = v
+    if storage == "f32":
+        for st in ("f16", "bf16"):
+            if get(variants, st, "MLUPS"):
+                out[st + "_vs_f32"] = round(variants[st]["MLUPS"] / mlups, 3)
+    ref = get(variants, "reference_bc_f64")
+    if ref:
+        out["reference_bc_f64"] = {"MLUPS": ref["MLUPS"], "step_kernel_frac": ref["step_kernel_frac"],
+                                   "e2e_MLUPS": get(ref, "e2e", "value")}
+    for tau in PRECISION_TAUS:
+        b = get(precision, "tau_%g" % tau)
+        if b:
+            out["precision_tau_%g" % tau] = {
+                "tawss_rel_l2": {"f32_vs_f64": get(b, "f32", "vs_f64", "tawss_rel_l2"),
+                                 "f16_vs_f64": get(b, "f16", "vs_f64", "tawss_rel_l2"),
+                                 "f16_vs_f32": get(b, "f16", "vs_f32", "tawss_rel_l2"),
+                                 "bf16_vs_f64": get(b, "bf16", "vs_f64", "tawss_rel_l2")},
+                "osi_abs_max": {"f32_vs_f64": get(b, "f32", "vs_f64", "osi_abs_max"),
+                                "f16_vs_f64": get(b, "f16", "vs_f64", "osi_abs_max"),
+                                "f16_vs_f32": get(b, "f16", "vs_f32", "osi_abs_max")}}
+    if adjoint:
+        out["adjoint_stenosed_pipe"] = {"cost_vs_forward_step": adjoint.get("cost_per_step_vs_forward_step"),
+                                        "f32_vs_fd_rel": adjoint.get("f32_vs_fd_rel"),
+                                        "f64_vs_fd_rel": adjoint.get("f64_vs_fd_rel")}
+    if configs:
+        out["aneurysm"] = {"f32_MLUPS": get(configs, "aneurysm", "f32", "MLUPS"),
+                           "f16_MLUPS": get(configs, "aneurysm", "f16", "MLUPS"),
+                           "adjoint_cost_vs_forward_step": get(configs, "aneurysm_adjoint",
+                                                               "cost_per_step_vs_forward_step")}
+        out["bifurcation_f32_MLUPS"] = get(configs, "bifurcation", "f32", "MLUPS")
+    if cpu:
+        out["cpu_reference_MLUPS"] = {"value": cpu.get("value"), "cores": cpu.get("cores"),
+                                      "cpu_model": cpu.get("cpu_model")}
+    return out
 
 
 def end_to_end(eng, n, Q, steps, torch):
@@ -370,6 +435,19 @@ def run_variants(args, topo, n, torch, device, vel, radius):
                               "step_kernel_GBs": round(2 * 19 * 4 * n / (ms_step / steps / 1e3) / 1e9, 1),
                               "device_flags": eng.flags()}
     eng.close()
+    # like for like with the reference arm: FP64 storage and arithmetic, the
+    # reference's boundary rules, same workload; kernel time and end to end
+    # through the C ABI from host buffers
+    peak, _ = measured_peaks()
+    eng, total_ms, ms_step, _ = time_engine(topo, "f64", steps, args.warmup, device, torch, vel, "reference",
+                                            radius)
+    gbs = 2 * 19 * 8 * n / (ms_step / steps / 1e3) / 1e9
+    out["reference_bc_f64"] = {"MLUPS": round(n * steps / (total_ms / 1e3) / 1e6, 1),
+                               "step_kernel_GBs": round(gbs, 1), "step_kernel_frac": round(gbs / peak, 4),
+                               "algorithmic_bytes_per_node": 2 * 19 * 8,
+                               "device_flags": eng.flags(),
+                               "e2e": None if args.no_e2e else end_to_end(eng, n, 19, steps, torch)}
+    eng.close()
     return out
 
 
@@ -387,12 +465,20 @@ def harmonic_waveform(seed=3, n=4):
     return amp, phase
 
 
+PRECISION_TAUS = (0.52, 0.55)
+
+
 def run_precision(torch, device, topo=None):
     """TAWSS / OSI (FP64 accumulators) and final-state errors of FP32, FP16 and
-    BF16 storage against FP64 storage, on the radius-20 tortuous vessel over
-    two periods of a 4-harmonic waveform (tau 0.52, Re 300 at the mean flow).
-    Errors are relative L2 norms over all near-wall nodes (TAWSS, WSS),
-    over all nodes (velocity, populations f - w), and max |OSI| differences."""
+    BF16 storage on the radius-20 tortuous vessel over two periods of a
+    4-harmonic waveform, at tau 0.52 (Re 300 at the mean flow, the precision
+    config) and at tau 0.55 (the same inflow, Re 120), where the flow no longer
+    amplifies every perturbation. Each storage type is compared with FP64
+    storage, and FP16 / BF16 also with FP32 storage, so that storage rounding
+    and the flow's sensitivity can be told apart. Errors are relative L2 norms
+    over all near-wall nodes (TAWSS, WSS), over all nodes (velocity,
+    populations f - w), the largest relative TAWSS difference (to the largest
+    TAWSS) and the largest absolute OSI difference."""
     from lbm_b200 import Engine
     from lbm_b200 import geometry as G
     r = 20.0
@@ -407,37 +493,45 @@ def run_precision(torch, device, topo=None):
     def l2(a, b):
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
+    def errors(a, b):
+        osi, tawss, wss, d, u = a
+        return {"tawss_rel_l2": l2(tawss, b[1]),
+                "tawss_rel_max": float(np.max(np.abs(tawss - b[1])) / np.max(np.abs(b[1]))),
+                "osi_abs_max": float(np.max(np.abs(osi - b[0]))),
+                "wss_rel_l2": l2(wss, b[2]), "velocity_rel_l2": l2(u, b[4]), "populations_rel_l2": l2(d, b[3])}
+
     out = {"workload": "tortuous stenosed vessel radius 20 lu, 512x512x1024 box (%d fluid nodes)" % n,
            "steps": steps, "waveform": {"period_steps": PRECISION_PERIOD, "amplitude": np.round(amp, 4).tolist(),
                                         "phase": np.round(phase, 4).tolist(), "seed": 3},
-           "tau": TAU, "mean_inlet_velocity": round(vel, 6)}
-    ref = None
-    for storage in ("f64", "f32", "f16", "bf16"):
-        eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device, bc="physics")
-        eng.set_inlet_profile(inlet_profile(topo, r, vel))
-        eng.set_waveform(float(PRECISION_PERIOD), amp, phase)
-        eng.set_flow(False, vel, harmonic=True)
-        t0 = time.perf_counter()
-        eng.step(steps)
-        osi, tawss = eng.osi_tawss()
-        wss = eng.wss()[0]
-        d = eng.populations() - w
-        u = eng.macros()[1]
-        flags = eng.flags()
-        secs = time.perf_counter() - t0
-        eng.close()
-        row = {"seconds": round(secs, 2), "device_flags": flags}
-        if ref is None:
-            ref = (osi, tawss, wss, d, u)
-            row["tawss_mean"] = float(np.mean(tawss))
-            row["osi_max"] = float(np.max(osi))
-        else:
-            row.update({"tawss_rel_l2": l2(tawss, ref[1]),
-                        "tawss_rel_max": float(np.max(np.abs(tawss - ref[1])) / np.max(np.abs(ref[1]))),
-                        "osi_abs_max": float(np.max(np.abs(osi - ref[0]))),
-                        "wss_rel_l2": l2(wss, ref[2]), "velocity_rel_l2": l2(u, ref[4]),
-                        "populations_rel_l2": l2(d, ref[3])})
-        out[storage] = row
+           "mean_inlet_velocity": round(vel, 6)}
+    for tau in PRECISION_TAUS:
+        res = {}
+        block = {"reynolds": round(vel * 2 * r / ((tau - 0.5) / 3.0), 1)}
+        for storage in ("f64", "f32", "f16", "bf16"):
+            eng = Engine(topo, tau=tau, dt=1e-5, spacing=1.0, storage=storage, device=device, bc="physics")
+            eng.set_inlet_profile(inlet_profile(topo, r, vel))
+            eng.set_waveform(float(PRECISION_PERIOD), amp, phase)
+            eng.set_flow(False, vel, harmonic=True)
+            t0 = time.perf_counter()
+            eng.step(steps)
+            osi, tawss = eng.osi_tawss()
+            wss = eng.wss()[0]
+            d = eng.populations() - w
+            u = eng.macros()[1]
+            flags = eng.flags()
+            secs = time.perf_counter() - t0
+            eng.close()
+            res[storage] = (osi, tawss, wss, d, u)
+            row = {"seconds": round(secs, 2), "device_flags": flags}
+            if storage == "f64":
+                row["tawss_mean"] = float(np.mean(tawss))
+                row["osi_max"] = float(np.max(osi))
+            else:
+                row["vs_f64"] = errors(res[storage], res["f64"])
+                if storage != "f32":
+                    row["vs_f32"] = errors(res[storage], res["f32"])
+            block[storage] = row
+        out["tau_%g" % tau] = block
     return out
 
 
@@ -783,7 +877,7 @@ def cpu_reference(args, sample_only=False, steps=None, procs=None):
     # all processes run concurrently: aggregate = nodes / slowest wall time
     slowest = max(r["seconds"] for r in results)
     value = sum(r["nodes"] for r in results) * steps / slowest / 1e6
-    return {"value": round(value, 4), "unit": "MLUPS", "cores": procs, "kind": "reference",
+    return {"value": round(value, 4), "unit": "MLUPS", "cores": procs, "kind": "reference", **host_cpu(),
             "workload": desc, "inlet_velocity": round(vel, 6),
             "sample": "%d slab(s) of %d z-layers of the workload (%d nodes), %d steps each, "
                       "reference Simulation step methods, serial MPI build"

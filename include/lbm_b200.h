@@ -128,8 +128,18 @@ int lbm_set_outlet_density(lbm_engine* e, double rho);
 /* Runs n_steps time steps: for each, the work of Collision, Streaming,
  * ApplyZouHeBc, ApplyOutletBc, ApplyWallBc, ComputeWallShearStress
  * (Simulation.cpp:553-568). Asynchronous on the engine's stream; results
- * below synchronise. */
+ * below synchronise.
+ * Numeric faults: behind every 256 steps (and at the end of the call) the
+ * device flags are copied to the host without waiting for them. With the
+ * numeric check on (the default), once such a copy has arrived showing a
+ * non-finite density (lbm_get_flags bit 2), lbm_step runs no further steps and
+ * returns LBM_ERR_NUMERIC; the steps taken before stay taken (lbm_get_time).
+ * The reference has no such check (it runs on with NaN and inf values). */
 int lbm_step(lbm_engine* e, int64_t n_steps);
+
+/* Numeric check of lbm_step (default 1): 0 runs on through non-finite values,
+ * as the reference does. */
+int lbm_set_numeric_check(lbm_engine* e, int32_t enabled);
 
 /* Observation policy (default 1). With 1, the last two steps of every
  * lbm_step call also store the state the getters read (populations, density
@@ -147,7 +157,7 @@ int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime);
 int lbm_get_populations(lbm_engine* e, double* f);
 
 /* Replaces the populations (the state after the current step); the next
- * step collides them. */
+ * step collides them. Clears the device flags and the numeric-fault state. */
 int lbm_set_populations(lbm_engine* e, const double* f);
 
 /* Node::density and Node::velocity after the last step: the moments the
@@ -188,15 +198,20 @@ int lbm_get_flux(lbm_engine* e, double* inlet, double* outlets);
  * partial sums go to a fixed 32 KiB device array inside the library, so
  * n_list may not exceed LBM_FLUX_NOALLOC_MAX_NODES (longer lists are rejected
  * with LBM_ERR_ARGUMENT). Runs asynchronously on `stream` (a cudaStream_t, NULL
- * for the default stream). The first call on a device looks up that array's
- * device address; make it outside any stream capture. Every call on a device
- * shares the array, so calls that overlap on the GPU race. List entries
- * outside [0, n_nodes) contribute nothing. Errors: lbm_last_error(NULL). */
+ * for the default stream) of the current device. The array belongs to the
+ * library's device code, which CUDA loads (by default lazily) on the first
+ * call on each device: that call is where the driver allocates the array, so
+ * a caller that may not allocate later makes a first call at start-up (n_list
+ * = 0 is enough; it writes 0 to *flux), outside any stream capture. Every call
+ * on a device shares the array, so calls that overlap on the GPU race. List
+ * entries outside [0, n_nodes) contribute nothing. Errors:
+ * lbm_last_error(NULL). */
 int lbm_flux_noalloc(const double* f, int64_t n_nodes, int32_t q, const int64_t* nodes, int64_t n_list,
                      const double normal[3], double* flux, void* stream);
 
-/* Device status bits since creation: 1 = a streamed population was exactly
- * zero (the reference would not have streamed it), 2 = non-finite density. */
+/* Device status bits since creation or the last lbm_set_populations: 1 = a
+ * streamed population was exactly zero (the reference would not have streamed
+ * it), 2 = non-finite density. */
 int lbm_get_flags(lbm_engine* e, uint32_t* flags);
 
 /* Runs n_steps steps like lbm_step and returns their device time per kernel
@@ -297,10 +312,16 @@ typedef struct lbm_voxel lbm_voxel;
 
 /* Reads an ASCII STL with the line grammar of Reader::readSTLASCII into a
  * malloc'd [n][12] array (layout of lbm_voxel_desc.triangles); release it
- * with lbm_free. */
+ * with lbm_free. Where the reference silently skips a malformed facet (or
+ * reuses the previous facet's vertices), this returns LBM_ERR_ARGUMENT with
+ * the file and line: a facet that breaks the grammar, a file that ends inside
+ * a facet, a file without facets. */
 int lbm_stl_read_ascii(const char* path, int64_t* n_triangles, double** triangles);
 void lbm_free(void* p);
 
+/* LBM_ERR_ARGUMENT where the reference only warns (ComplexGeometry.cpp:
+ * 664-692) and goes on to a simulation nothing drives: no inlet opening, or
+ * inlet openings that match no grid point. */
 int lbm_voxelise(const lbm_voxel_desc* desc, lbm_voxel** out);
 /* Grid points per axis, grid origin (bounding-box minimum), spacing, node and
  * near-wall counts, wall-clock build time (ms). Any may be NULL. */

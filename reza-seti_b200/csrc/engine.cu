@@ -353,6 +353,14 @@ struct lbm_engine {
     double* staging = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> evpool;
+    // numeric-fault detection (lbm_set_numeric_check): the device flags are
+    // copied into pinned host memory behind the steps and read once that copy
+    // has completed, so the check never waits for the GPU
+    bool numeric_check = true;
+    unsigned* flag_host = nullptr;     // pinned mirror of *flags
+    cudaEvent_t flag_ev = nullptr;     // recorded after the mirror's copy
+    bool flag_copy_pending = false;
+    bool numeric_fault = false;        // a completed copy showed FLAG_NONFINITE
 
     template <class T>
     cudaError_t alloc(T** p, size_t count) {
@@ -526,6 +534,51 @@ int init_from_obs(lbm_engine* e) {
     return 0;
 }
 
+// Reads the flag mirror if its copy has completed (never blocks).
+void poll_flags(lbm_engine* e) {
+    if (!e->flag_copy_pending) return;
+    const cudaError_t q = cudaEventQuery(e->flag_ev);
+    if (q == cudaErrorNotReady) return;
+    if (q != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    e->flag_copy_pending = false;
+    if (*e->flag_host & FLAG_NONFINITE) e->numeric_fault = true;
+}
+
+// Queues a copy of the device flags into the mirror behind the work issued so
+// far (one copy in flight at a time).
+void post_flags(lbm_engine* e) {
+    if (e->flag_copy_pending) return;
+    if (cudaMemcpyAsync(e->flag_host, e->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+        cudaEventRecord(e->flag_ev, e->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    e->flag_copy_pending = true;
+}
+
+// Steps between two flag copies inside one lbm_step call.
+constexpr int64_t FLAG_POLL_STEPS = 256;
+
+// LBM_ERR_NUMERIC once a completed copy of the device flags showed
+// non-finite densities (when the check is on).
+int numeric_status(lbm_engine* e) {
+    if (!e->numeric_check) return 0;
+    poll_flags(e);
+    if (!e->numeric_fault) return 0;
+    return e->fail(LBM_ERR_NUMERIC, "non-finite densities reported by the device by step " + std::to_string(e->step) +
+                                        " (lbm_set_numeric_check(e, 0) runs on regardless)");
+}
+
+// Observation bits of a step followed by `left` more steps of its call: the
+// last two steps write the moments, the last one the populations too.
+int observe_bits(const lbm_engine* e, int64_t left) {
+    if (!e->observe) return 0;
+    return (left <= 1 ? 2 : 0) | (left == 0 ? 1 : 0);
+}
+
 // Physics mode: per step the stream+collide kernel, then one post-pass with
 // that step's wall shear stress and the open-boundary corrections of its
 // store (which streams into the next step). No pre-pass: physics mode has no
@@ -533,14 +586,12 @@ int init_from_obs(lbm_engine* e) {
 // ev[2i+1] before its post-pass; ev[2n] after the last post-pass. A WSS
 // hand-off left pending by an earlier reference-style sequence is reduced
 // first (never the case in physics mode, where every post-pass reduces it).
-int run_steps_physics(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
+int run_steps_physics(lbm_engine* e, int64_t n_steps, int64_t after, double* t_step, double* t_bnd) {
     const bool timed = t_step || t_bnd;
     const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
     for (int64_t i = 0; i < n_steps; ++i) {
         const int64_t t = e->step + 1;
-        int obs = 0;
-        if (e->observe && i >= n_steps - 2) obs |= 2;
-        if (e->observe && i == n_steps - 1) obs |= 1;
+        const int obs = observe_bits(e, n_steps - 1 - i + after);
         double* mom = e->obs_mom[t % 2];
         const int phase = e->phase;
         const double scale = inlet_factor(e, e->step + 1, pulsatile ? e->runtime + e->dt : e->runtime);
@@ -588,8 +639,34 @@ int run_steps_physics(lbm_engine* e, int64_t n_steps, double* t_step, double* t_
     return 0;
 }
 
+int run_steps_checked(lbm_engine* e, int64_t n_steps, int64_t after, double* t_step, double* t_bnd);
+
+// Runs n_steps steps in chunks of FLAG_POLL_STEPS with a flag copy behind each
+// chunk; with the numeric check on, stops before the next chunk once a copy
+// that has completed shows non-finite densities.
 int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
     if (n_steps < 0) return e->fail(LBM_ERR_ARGUMENT, "negative step count");
+    if (int rc = numeric_status(e)) return rc;
+    if (t_step || t_bnd) {
+        // timed runs are one chunk: their events are read once at the end
+        const int rc = run_steps_checked(e, n_steps, 0, t_step, t_bnd);
+        post_flags(e);
+        return rc;
+    }
+    for (int64_t done = 0; done < n_steps;) {
+        const int64_t chunk = std::min<int64_t>(FLAG_POLL_STEPS, n_steps - done);
+        if (int rc = run_steps_checked(e, chunk, n_steps - done - chunk, nullptr, nullptr)) return rc;
+        done += chunk;
+        post_flags(e);
+        if (done < n_steps)
+            if (int rc = numeric_status(e)) return rc;
+    }
+    return 0;
+}
+
+// `after`: steps of the same lbm_step call that follow these (the call's
+// last two steps are the observed ones).
+int run_steps_checked(lbm_engine* e, int64_t n_steps, int64_t after, double* t_step, double* t_bnd) {
     if (n_steps == 0) return 0;
     if (t_step) *t_step = 0;
     if (t_bnd) *t_bnd = 0;
@@ -607,16 +684,14 @@ int run_steps(lbm_engine* e, int64_t n_steps, double* t_step, double* t_bnd) {
             e->evpool.push_back(ev);
         }
     }
-    if (e->bc == LBM_BC_PHYSICS) return run_steps_physics(e, n_steps, t_step, t_bnd);
+    if (e->bc == LBM_BC_PHYSICS) return run_steps_physics(e, n_steps, after, t_step, t_bnd);
     for (int64_t i = 0; i < n_steps; ++i) {
         const int64_t t = e->step + 1;
         const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
         // reference-mode inlet velocity of this step (Simulation.cpp:558-562)
         const double vel = pulsatile ? pulsatile_at(e, e->runtime)
                                      : e->cte_vel * inlet_factor(e, e->step, e->runtime);
-        int obs = 0;
-        if (e->observe && i >= n_steps - 2) obs |= 2;
-        if (e->observe && i == n_steps - 1) obs |= 1;
+        const int obs = observe_bits(e, n_steps - 1 - i + after);
         double* mom = e->obs_mom[t % 2];
         const int phase = e->phase;
         int rc = dispatch(e, [&](auto tag) {
@@ -685,6 +760,7 @@ int sync(lbm_engine* e) {
     cudaError_t ce = cudaStreamSynchronize(e->stream);
     return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "stream synchronize");
 }
+
 
 int create(const lbm_desc* d, lbm_engine** out) {
     if (!d || !out) {
@@ -759,6 +835,10 @@ int create(const lbm_desc* d, lbm_engine** out) {
     e->own_stream = true;
     for (auto& ev : e->ev)
         if ((ce = cudaEventCreate(&ev)) != cudaSuccess) return bail(ce, "event");
+    if ((ce = cudaEventCreateWithFlags(&e->flag_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(ce, "event");
+    if ((ce = cudaHostAlloc((void**)&e->flag_host, sizeof(unsigned), cudaHostAllocDefault)) != cudaSuccess)
+        return bail(ce, "flag mirror");
+    *e->flag_host = 0;
 
     const Topo& t = e->t;
     const size_t elem = e->storage == LBM_STORE_F64 ? 8 : (e->storage == LBM_STORE_F32 ? 4 : 2);
@@ -864,6 +944,8 @@ int lbm_destroy(lbm_engine* e) {
     for (auto& ev : e->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : e->evpool) cudaEventDestroy(ev);
+    if (e->flag_ev) cudaEventDestroy(e->flag_ev);
+    if (e->flag_host) cudaFreeHost(e->flag_host);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;
     return 0;
@@ -893,14 +975,15 @@ int lbm_set_pulsatile(lbm_engine* e, const lbm_pulse_desc* w) {
     if (!e) return LBM_ERR_ARGUMENT;
     if (!w) {
         e->pulse_custom = false;
-        return LBM_OK;
+        return reapply_initial_store(e);
     }
     lbm::Pulse p;
     const std::string err = lbm::pulse_from_desc(*w, p);
     if (!err.empty()) return e->fail(LBM_ERR_ARGUMENT, err);
     e->pulse = std::move(p);
     e->pulse_custom = true;
-    return LBM_OK;
+    // the inlet correction of the initial store reads the waveform at t = 0
+    return reapply_initial_store(e);
 }
 
 int lbm_set_waveform(lbm_engine* e, double period_steps, int32_t n_harmonics, const double* amplitude,
@@ -938,6 +1021,12 @@ int lbm_set_outlet_density(lbm_engine* e, double rho) {
     if (!e) return LBM_ERR_ARGUMENT;
     e->out_rho = rho;
     return reapply_initial_store(e);
+}
+
+int lbm_set_numeric_check(lbm_engine* e, int32_t enabled) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    e->numeric_check = enabled != 0;
+    return 0;
 }
 
 int lbm_set_observation(lbm_engine* e, int32_t enabled) {
@@ -985,6 +1074,12 @@ int lbm_set_populations(lbm_engine* e, const double* f) {
     if (!e || !f) return LBM_ERR_ARGUMENT;
     cudaSetDevice(e->device);
     if (int rc = ensure_staging(e)) return rc;
+    // a new state: the device flags and the numeric-fault state start afresh
+    if (int rc = sync(e)) return rc;
+    e->flag_copy_pending = false;
+    e->numeric_fault = false;
+    cudaError_t cm = cudaMemsetAsync(e->flags, 0, sizeof(unsigned), e->stream);
+    if (cm != cudaSuccess) return e->cuda_fail(cm, "flags");
     cudaError_t ce = cudaMemcpyAsync(e->staging, f, sizeof(double) * e->t.n * e->Q, cudaMemcpyHostToDevice, e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "upload");
     ce = launch_pop_from_caller(e->staging, e->perm, e->t.n, e->Q, e->t.ld, e->obs_pop, e->stream);
@@ -1051,11 +1146,11 @@ int lbm_get_flux(lbm_engine* e, double* inlet, double* outlets) {
     if (e->pop_step != e->step) return e->fail(LBM_ERR_STATE, "populations of the last step were not observed");
     cudaSetDevice(e->device);
     const int n_out = (int)e->t.out_normal.size() / 3;
-    cudaError_t ce = launch_flux(e->Q, e->obs_pop, 1, e->t.ld, e->flux_nodes, e->nin(), e->inlet_normal,
+    cudaError_t ce = launch_flux(e->Q, e->obs_pop, 1, e->t.ld, e->t.n, e->flux_nodes, e->nin(), e->inlet_normal,
                                  e->flux_partials, e->flux_out, e->stream);
     for (int o = 0; o < n_out && ce == cudaSuccess; ++o) {
         const long long b = e->t.out_off[o], n = e->t.out_off[o + 1] - b;
-        ce = launch_flux(e->Q, e->obs_pop, 1, e->t.ld, e->flux_nodes + e->nin() + b, n, &e->t.out_normal[3 * o],
+        ce = launch_flux(e->Q, e->obs_pop, 1, e->t.ld, e->t.n, e->flux_nodes + e->nin() + b, n, &e->t.out_normal[3 * o],
                          e->flux_partials, e->flux_out + 1 + o, e->stream);
     }
     if (ce != cudaSuccess) return e->cuda_fail(ce, "flux kernels");

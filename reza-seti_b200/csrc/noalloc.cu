@@ -8,19 +8,26 @@
 // holds populations in someone else's buffers and wants the inlet/outlet flux
 // without creating an engine (lbm_create allocates the whole lattice).
 //
-// How: the same two-stage FP64 reduction as lbm_get_flux (reduce.cuh: warp
-// shuffles, one partial sum per block, one block summing the partials), but
-// the partial sums go to g_flux_partials, a fixed array in this file's device
-// memory, instead of engine-allocated scratch. The array exists on
-// every device that loads the library, until the process exits. Its size
-// bounds the list length: LBM_FLUX_NOALLOC_MAX_NODES entries (4096 blocks of
-// 256, 32 KiB). The caller passes the populations, the node list and the
-// result location, all in device memory.
+// How: the kernels of lbm_get_flux itself (reduce.cuh: warp shuffles, one
+// partial sum per block, one block summing the partials, so both entry points
+// sum in the same order), reading the caller's [node][q] populations through
+// strides, with the partial sums in g_flux_partials, a fixed array in this
+// file's device memory, instead of engine-allocated scratch. Its size bounds
+// the list length: LBM_FLUX_NOALLOC_MAX_NODES entries (4096 blocks of 256,
+// 32 KiB). The caller passes the populations, the node list and the result
+// location, all in device memory.
+//
+// The array is part of the library's device code. Under lazy module loading
+// (the CUDA default) the driver loads that code, and allocates the array with
+// it, on the first call on each device; a caller that may not allocate later
+// makes that first call (n_list = 0 is enough) at start-up, outside any stream
+// capture. The array then stays on that device until the process exits.
 //
 // Host code never dereferences g_flux_partials: on the host its name is only a
-// stand-in for the symbol. The first call on each device resolves the array's
-// device address with cudaGetSymbolAddress (with that device current) and
-// caches it; make that first call outside any stream capture.
+// stand-in for the symbol. Every call looks the array's device address up with
+// cudaGetSymbolAddress, with the caller's device current: the lookup allocates
+// nothing, and a cached address could outlive the context it belongs to (after
+// cudaDeviceReset).
 //
 // Shared state: every call on a device uses the same array, which keeps the
 // previous call's partial sums. Nothing needs clearing — each call writes one
@@ -28,101 +35,23 @@
 // overlap on the GPU (different streams, no ordering) race on the array.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
-#include <vector>
 
 #include "errors.h"
-#include "lattice.cuh"
 #include "lbm_b200.h"
+#include "reduce.cuh"
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kMaxBlocks = (int)(LBM_FLUX_NOALLOC_MAX_NODES / kThreads);
-static_assert((long long)kMaxBlocks * kThreads == LBM_FLUX_NOALLOC_MAX_NODES,
+constexpr int kMaxBlocks = (int)(LBM_FLUX_NOALLOC_MAX_NODES / lbm::FLUX_THREADS);
+static_assert((long long)kMaxBlocks * lbm::FLUX_THREADS == LBM_FLUX_NOALLOC_MAX_NODES,
               "the list limit must be a whole number of blocks");
 
 static __device__ __align__(256) double g_flux_partials[kMaxBlocks];
 
-std::mutex g_mu;
-std::vector<double*> g_partials_ptr;  // device address of g_flux_partials per device ordinal
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// One partial sum per block of the caller's list, populations laid out
-// [node][q]; entries outside [0, n_nodes) contribute nothing (the list lives
-// in device memory the host cannot check).
-template <int Q>
-__global__ void __launch_bounds__(kThreads) flux_partial_noalloc_kernel(
-    const double* __restrict__ f, long long n_nodes, const long long* __restrict__ nodes, long long n_list,
-    double nx, double ny, double nz, double* partials) {
-    using L = lbm::Lat<Q>;
-    __shared__ double warp_part[kThreads / 32];
-    const long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
-    double v = 0.0;
-    if (i < n_list) {
-        const long long node = nodes[i];
-        if (node >= 0 && node < n_nodes) {
-            const double* p = f + node * Q;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const double cn = L::cx(q) * nx + L::cy(q) * ny + L::cz(q) * nz;
-                if (L::cx(q) || L::cy(q) || L::cz(q)) v += cn * p[q];
-            }
-        }
-    }
-    v = warp_sum(v);
-    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double w = threadIdx.x < kThreads / 32 ? warp_part[threadIdx.x] : 0.0;
-        w = warp_sum(w);
-        if (threadIdx.x == 0) partials[blockIdx.x] = w;
-    }
-}
-
-// Sum of the first n_partials partial sums into *out.
-__global__ void __launch_bounds__(kThreads) flux_final_noalloc_kernel(const double* __restrict__ partials,
-                                                                      int n_partials, double* out) {
-    __shared__ double warp_part[kThreads / 32];
-    double v = 0.0;
-    for (int i = threadIdx.x; i < n_partials; i += kThreads) v += partials[i];
-    v = warp_sum(v);
-    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double w = threadIdx.x < kThreads / 32 ? warp_part[threadIdx.x] : 0.0;
-        w = warp_sum(w);
-        if (threadIdx.x == 0) *out = w;
-    }
-}
-
 int fail(int code, const std::string& msg) {
     lbm::set_global_error("lbm_flux_noalloc: " + msg);
     return code;
-}
-
-// Device address of this device's partial-sum array (set-up on first use).
-int partials_for_current_device(double** out) {
-    int dev = 0;
-    cudaError_t ce = cudaGetDevice(&dev);
-    if (ce != cudaSuccess) return fail(LBM_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
-    std::lock_guard<std::mutex> lock(g_mu);
-    if ((int)g_partials_ptr.size() <= dev) g_partials_ptr.resize(dev + 1, nullptr);
-    if (!g_partials_ptr[dev]) {
-        void* p = nullptr;
-        ce = cudaGetSymbolAddress(&p, g_flux_partials);
-        if (ce != cudaSuccess)
-            return fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
-        g_partials_ptr[dev] = static_cast<double*>(p);
-    }
-    *out = g_partials_ptr[dev];
-    return LBM_OK;
 }
 
 }  // namespace
@@ -136,21 +65,12 @@ extern "C" int lbm_flux_noalloc(const double* f, int64_t n_nodes, int32_t q, con
         return fail(LBM_ERR_ARGUMENT, "list of " + std::to_string(n_list) + " nodes exceeds the maximum of " +
                                           std::to_string((long long)LBM_FLUX_NOALLOC_MAX_NODES) +
                                           " (LBM_FLUX_NOALLOC_MAX_NODES)");
-    double* partials = nullptr;
-    if (int rc = partials_for_current_device(&partials)) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int blocks = (int)((n_list + kThreads - 1) / kThreads);
-    const long long* nl = reinterpret_cast<const long long*>(nodes);
-    if (blocks > 0) {
-        if (q == 19)
-            flux_partial_noalloc_kernel<19><<<blocks, kThreads, 0, st>>>(f, n_nodes, nl, n_list, normal[0],
-                                                                         normal[1], normal[2], partials);
-        else
-            flux_partial_noalloc_kernel<27><<<blocks, kThreads, 0, st>>>(f, n_nodes, nl, n_list, normal[0],
-                                                                         normal[1], normal[2], partials);
-    }
-    flux_final_noalloc_kernel<<<1, kThreads, 0, st>>>(partials, blocks, flux);
-    cudaError_t ce = cudaGetLastError();
+    void* partials = nullptr;
+    cudaError_t ce = cudaGetSymbolAddress(&partials, g_flux_partials);
+    if (ce != cudaSuccess) return fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
+    // the caller's layout [node][q]: stride q between nodes, 1 between directions
+    ce = lbm::launch_flux(q, f, q, 1, n_nodes, reinterpret_cast<const long long*>(nodes), n_list, normal,
+                          static_cast<double*>(partials), flux, static_cast<cudaStream_t>(stream));
     if (ce != cudaSuccess) return fail(LBM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(ce));
     return LBM_OK;
 }

@@ -410,44 +410,52 @@ int lbm_stl_read_ascii(const char* path, int64_t* n_triangles, double** triangle
         return LBM_ERR_ARGUMENT;
     }
     // the line grammar of Reader::readSTLASCII: "facet normal nx ny nz",
-    // "outer loop", three "vertex x y z", "endloop", "endfacet"; a facet whose
-    // lines do not follow it is skipped
+    // "outer loop", three "vertex x y z", "endloop", "endfacet". The
+    // reference skips a facet whose lines do not follow it (and keeps the
+    // previous facet's vertices where a vertex line fails), without a word;
+    // here a facet that does not follow it, or a file that ends inside one,
+    // is an error naming the line, and so is a file without facets.
     std::vector<double> out;
     std::string line, w1, w2;
-    while (std::getline(file, line)) {
-        std::stringstream ss(line);
+    long long lineno = 0;
+    auto bad = [&](const char* what) {
+        lbm::set_global_error(std::string(path) + ":" + std::to_string(lineno) + ": " + what);
+        return LBM_ERR_ARGUMENT;
+    };
+    auto next = [&](std::stringstream& ss) {
+        if (!std::getline(file, line)) return false;
+        ++lineno;
+        ss.clear();
+        ss.str(line);
+        return true;
+    };
+    std::stringstream ss;
+    while (next(ss)) {
         double n[3];
-        if (!(ss >> w1 >> w2 >> n[0] >> n[1] >> n[2]) || w1 != "facet" || w2 != "normal") continue;
-        if (!std::getline(file, line)) break;
-        ss.clear();
-        ss.str(line);
-        if (!(ss >> w1 >> w2) || w1 != "outer" || w2 != "loop") continue;
+        if (!(ss >> w1) || w1 != "facet") continue;  // solid / endsolid / blank lines
+        if (!(ss >> w2 >> n[0] >> n[1] >> n[2]) || w2 != "normal") return bad("malformed facet normal line");
+        if (!next(ss)) return bad("file ends inside a facet");
+        if (!(ss >> w1 >> w2) || w1 != "outer" || w2 != "loop") return bad("expected outer loop");
         double v[9];
-        bool ok = true;
-        for (int i = 0; i < 3 && ok; ++i) {
-            if (!std::getline(file, line)) {
-                ok = false;
-                break;
-            }
-            ss.clear();
-            ss.str(line);
-            ok = (ss >> w1 >> v[3 * i] >> v[3 * i + 1] >> v[3 * i + 2]) && w1 == "vertex";
+        for (int i = 0; i < 3; ++i) {
+            if (!next(ss)) return bad("file ends inside a facet");
+            if (!(ss >> w1 >> v[3 * i] >> v[3 * i + 1] >> v[3 * i + 2]) || w1 != "vertex")
+                return bad("malformed vertex line");
         }
-        if (!std::getline(file, line)) break;
-        ss.clear();
-        ss.str(line);
-        if (!(ss >> w1) || w1 != "endloop") continue;
-        if (!std::getline(file, line)) break;
-        ss.clear();
-        ss.str(line);
-        if (!(ss >> w1) || w1 != "endfacet") continue;
-        if (!ok) continue;
+        if (!next(ss)) return bad("file ends inside a facet");
+        if (!(ss >> w1) || w1 != "endloop") return bad("expected endloop");
+        if (!next(ss)) return bad("file ends inside a facet");
+        if (!(ss >> w1) || w1 != "endfacet") return bad("expected endfacet");
         for (int i = 0; i < 9; ++i) out.push_back(v[i]);
         for (int i = 0; i < 3; ++i) out.push_back(n[i]);
     }
-    double* buf = (double*)std::malloc(std::max<size_t>(out.size(), 1) * sizeof(double));
+    if (out.empty()) {
+        lbm::set_global_error(std::string(path) + ": no facets");
+        return LBM_ERR_ARGUMENT;
+    }
+    double* buf = (double*)std::malloc(out.size() * sizeof(double));
     if (!buf) return LBM_ERR_ARGUMENT;
-    if (!out.empty()) std::memcpy(buf, out.data(), out.size() * sizeof(double));
+    std::memcpy(buf, out.data(), out.size() * sizeof(double));
     *triangles = buf;
     *n_triangles = (int64_t)(out.size() / 12);
     return LBM_OK;
@@ -517,6 +525,9 @@ int lbm_voxelise(const lbm_voxel_desc* d, lbm_voxel** out) {
         ops.push_back(op);
     }
     if (n_out > 255) return fail(LBM_ERR_ARGUMENT, "too many outlets");
+    // the reference only warns (ComplexGeometry.cpp:667-672) and then runs a
+    // simulation that nothing drives
+    if (!last_inlet) return fail(LBM_ERR_ARGUMENT, "no inlet opening given");
 
     DevBufs B;
     Tri* d_tris = B.get<Tri>(nt);
@@ -602,6 +613,11 @@ int lbm_voxelise(const lbm_voxel_desc* d, lbm_voxel** out) {
             }
             if (near[i]) v->nearwall.push_back(i);
         }
+    }
+    if (v->inlet.empty()) {
+        delete v;
+        return fail(LBM_ERR_ARGUMENT, "the inlet opening matches no grid point (check its plane and coordinate "
+                                      "against the STL's bounding box)");
     }
     v->n_outlets = n_out;
     v->outlet_offsets.push_back(0);

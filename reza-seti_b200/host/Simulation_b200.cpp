@@ -267,6 +267,8 @@ Simulation::Simulation(SubDomain& SubDomain, SimulationParameters& simParams) : 
     d.dt = m_dt;
     d.spacing = SubDomain_.Geometry_.spacing;
     check(lbm_create(&d, &st.e), nullptr, "lbm_create");
+    // the reference runs on through non-finite values (no check in Iterate)
+    check(lbm_set_numeric_check(st.e, 0), st.e, "lbm_set_numeric_check");
     if (simParams.FlowType == "Pulsatile") set_waveform_from_equations(st.e, simParams, ext);
     Iterate();
 }

@@ -133,6 +133,7 @@ SIGNATURES = {
     "lbm_set_outlet_density": (ctypes.c_int, [_E, ctypes.c_double]),
     "lbm_step": (ctypes.c_int, [_E, ctypes.c_int64]),
     "lbm_set_observation": (ctypes.c_int, [_E, ctypes.c_int32]),
+    "lbm_set_numeric_check": (ctypes.c_int, [_E, ctypes.c_int32]),
     "lbm_get_time": (ctypes.c_int, [_E, _i64p, _f64p]),
     "lbm_get_populations": (ctypes.c_int, [_E, ctypes.c_void_p]),
     "lbm_set_populations": (ctypes.c_int, [_E, ctypes.c_void_p]),

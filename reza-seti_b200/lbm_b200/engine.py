@@ -39,7 +39,7 @@ class Engine:
     """One engine on one GPU."""
 
     def __init__(self, topo, *, tau, dt=1e-5, spacing=1.0, lattice=19, storage="f64",
-                 bc="reference", device=0):
+                 bc="reference", device=0, numeric_check=True):
         L = capi.lib()
         self.q = lattice
         keep = {}
@@ -87,6 +87,8 @@ class Engine:
         self._h = h
         self._keep = keep
         self.tau, self.dt, self.spacing = float(tau), float(dt), float(spacing)
+        if not numeric_check:
+            self.set_numeric_check(False)
 
     # ---- lifecycle
     def close(self):
@@ -129,6 +131,12 @@ class Engine:
 
     def set_outlet_density(self, rho):
         self._check(capi.lib().lbm_set_outlet_density(self._h, float(rho)))
+
+    def set_numeric_check(self, enabled):
+        """With the check on (default), step() raises LbmError with code
+        LBM_ERR_NUMERIC once the device has reported non-finite densities;
+        off, it runs on through them as the reference does."""
+        self._check(capi.lib().lbm_set_numeric_check(self._h, 1 if enabled else 0))
 
     def set_observation(self, enabled):
         self._check(capi.lib().lbm_set_observation(self._h, 1 if enabled else 0))
@@ -253,9 +261,10 @@ class Simulation:
 
     def __init__(self, topo, params, storage="f64", on_output=None, device=0):
         self.params = dict(params)
+        # the reference runs on through non-finite values
         self.engine = Engine(topo, tau=params["tau"], dt=params.get("dt", 1e-5),
                              spacing=params.get("spacing", 1.0), storage=storage,
-                             bc="reference", device=device)
+                             bc="reference", device=device, numeric_check=False)
         self.pulsatile = params.get("FlowType", "Constant") == "Pulsatile"
         self.engine.set_flow(self.pulsatile, params.get("CteVel", 0.0))
         self.on_output = on_output

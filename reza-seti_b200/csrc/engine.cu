@@ -308,6 +308,7 @@ struct lbm_engine {
     double runtime = 0.0;
     int phase = 1;
     bool observe = true;       // lbm_set_observation
+    bool force_general = false;  // LBM_B200_PHASE1_GENERAL=1: phase-1 pair kernel without its twin path
     int64_t mom_step[2] = {-1, -1};  // step whose collision-input moments each obs_mom buffer holds
     int64_t pop_step = -1;           // step whose post-boundary populations obs_pop holds
     bool wss_pending = false;  // a step kernel handed near-wall populations not yet reduced to WSS
@@ -428,6 +429,7 @@ StepArgs<S, Q> step_args(lbm_engine* e, double vel, double* mom) {
     a.obs_pop = e->obs_pop;
     a.obs_mom = mom;
     a.flags = e->flags;
+    a.force_general = e->force_general ? 1 : 0;
     return a;
 }
 
@@ -807,6 +809,11 @@ int create(const lbm_desc* d, lbm_engine** out) {
     e->omega = 1.0 / d->tau;
     e->dt = d->dt;
     e->spacing = d->spacing;
+    {
+        // tests compare the phase-1 pair kernel's twin and per-node paths
+        const char* g = getenv("LBM_B200_PHASE1_GENERAL");
+        e->force_general = g && !strcmp(g, "1");
+    }
     {
         // Simulation::ComputeWallShearStress, Simulation.cpp:768-771
         const double phys_den = 1060;

@@ -111,6 +111,9 @@ struct StepArgs {
     double* obs_pop;       // [Q][ld] post-boundary populations f (natural layout)
     double* obs_mom;       // [4][ld] rho, ux, uy, uz
     unsigned* flags;
+    // phase-1 pair kernel: 1 = every warp takes the per-node path, never the
+    // twin path (LBM_B200_PHASE1_GENERAL=1; the two give identical results)
+    int force_general;
 };
 
 template <class S, int Q>

@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_p
         // mask address each direction once for both nodes
         const bool twin = ((m0 ^ m1) & Meta<Q>::mask_all()) == 0 &&
                           (m0 >> Meta<Q>::SEG_SHIFT) == (m1 >> Meta<Q>::SEG_SHIFT);
-        const bool uniform = __all_sync(0xffffffffu, twin);
+        const bool uniform = !a.force_general && __all_sync(0xffffffffu, twin);
         float2 s[Q];
         if (uniform) pair_gather1_twin<S, Q>(a, s, m0, sd0, n0);
         else pair_gather1<S, Q>(a, s, m0, m1, sd0, sd1, n0);

@@ -4,8 +4,13 @@ FP64 (reference boundary mode) must equal the reference solver's own dumps
 bit for bit: populations, density, velocity, WSS and its accumulators, after
 step 1 and after the last step of every golden case (every inlet / outlet
 branch of the reference, NaN-producing and diverging cases included). FP32
-storage must stay within 1e-5 of the FP64 oracle, normwise relative:
-max|a - b| / max|b| per field.
+storage must stay within 1e-5 relative of the FP64 oracle elementwise:
+|a - b| <= 1e-5 |b| + 3e-6 max|b| per field. The floor, 0.3 of the relative
+bound at the field's largest value, covers the components that are near zero
+(transverse velocities, WSS at low-shear nodes), which carry the absolute
+rounding error of the FP32 arithmetic; the 2000-step pipe needs 2.3e-6 of it
+for WSS, the short cases under 1e-7. Populations and densities pass without
+it.
 """
 import glob
 import os
@@ -25,6 +30,7 @@ STEPS = {"cyl_z": 60, "cyl_z_rev": 20, "cyl_x": 40, "cyl_x_rev": 20, "cyl_y": 4,
          "cyl_z_pulsatile": 100, "outlet_chain": 12}
 STABLE = ["cyl_z", "cyl_z_rev", "cyl_x", "cyl_x_rev", "outlet_chain"]
 FP32_RTOL = 1e-5
+FP32_FLOOR = 3e-6  # times max|b| of the field
 
 
 def load(path):
@@ -47,6 +53,13 @@ def same(a, b, what):
 def rel(a, b):
     den = np.max(np.abs(b))
     return float(np.max(np.abs(a - b)) / den) if den > 0 else float(np.max(np.abs(a - b)))
+
+
+def close(a, b, floor=FP32_FLOOR):
+    """|a - b| <= 1e-5 |b| + floor max|b| elementwise (the FP32 bound)."""
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    allow = FP32_RTOL * np.abs(b) + floor * np.max(np.abs(b))
+    return bool(np.all(np.abs(a - b) <= allow))
 
 
 @pytest.mark.parametrize("path", SMALL, ids=[os.path.basename(p)[:-4] for p in SMALL])
@@ -88,13 +101,14 @@ def test_fp32_within_1e5_of_oracle(name):
     o.run(STEPS[name], cte_vel=float(d["meta_d"][4]))
     e = engine_for(d, "f32")
     e.step(STEPS[name])
-    assert rel(e.populations(), o.f) <= FP32_RTOL
+    assert close(e.populations(), o.f, 0.0)
     rho, u = e.macros()
-    assert rel(u, o.u) <= FP32_RTOL
-    assert rel(rho, o.rho) <= FP32_RTOL
+    assert close(rho, o.rho, 0.0)
+    assert close(u, o.u)
     w, acc, accm = e.wss()
-    assert rel(w, o.wss) <= FP32_RTOL
-    assert rel(acc, o.acc) <= FP32_RTOL
+    assert close(w, o.wss)
+    assert close(acc, o.acc)
+    assert close(accm, o.accmag)
 
 
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
@@ -145,12 +159,14 @@ def test_pipe_2000_steps_against_reference():
     same(np.array([f.sum(), np.abs(f).sum(), (f * f).sum()]), d["final__f_sum"], "f sums")
     e32 = engine_for(d, "f32")
     e32.step(2000)
-    assert rel(e32.populations()[s], d["final__f_sample"]) <= FP32_RTOL
+    assert close(e32.populations()[s], d["final__f_sample"], 0.0)
     rho32, u32 = e32.macros()
-    assert rel(u32[s], d["final__u_sample"]) <= FP32_RTOL
-    w32, acc32, _ = e32.wss()
-    assert rel(w32, d["final__wss"]) <= FP32_RTOL
-    assert rel(acc32, d["final__acc"]) <= FP32_RTOL
+    assert close(rho32[s], d["final__rho_sample"], 0.0)
+    assert close(u32[s], d["final__u_sample"])
+    w32, acc32, accm32 = e32.wss()
+    assert close(w32, d["final__wss"])
+    assert close(acc32, d["final__acc"])
+    assert close(accm32, d["final__accmag"])
 
 
 def test_observation_switch():

@@ -87,16 +87,25 @@ def test_poiseuille_profile_and_mass_balance(q):
     assert inl < 0 and abs(inl + outs.sum()) < 5e-3 * abs(inl)
 
 
+def close(a, b, floor):
+    """|a - b| <= 1e-5 |b| + floor max|b|, elementwise."""
+    return bool(np.all(np.abs(a - b) <= 1e-5 * np.abs(b) + floor * np.max(np.abs(b))))
+
+
 @pytest.mark.parametrize("q", [19, 27])
 def test_fp32_storage_tracks_fp64(q):
+    """Elementwise 1e-5 relative on every population; on velocity and wall
+    shear stress above a floor of 1e-5 of the field's largest value (the
+    physics-mode FP32 traction uses the stress-tensor form, whose rounding
+    is absolute, and transverse velocities are near zero)."""
     topo = G.straight_pipe(radius=6.0, length=32)
     a = physics_engine(topo, 0.6, q=q, storage="f64")
     b = physics_engine(topo, 0.6, q=q, storage="f32")
     a.step(300)
     b.step(300)
-    assert rel(b.populations(), a.populations()) < 1e-5
-    assert rel(b.macros()[1], a.macros()[1]) < 1e-5
-    assert rel(b.wss()[0], a.wss()[0]) < 1e-4
+    assert close(b.populations(), a.populations(), 0.0)
+    assert close(b.macros()[1], a.macros()[1], 1e-5)
+    assert close(b.wss()[0], a.wss()[0], 1e-5)
 
 
 @pytest.mark.parametrize("q", [19, 27])

@@ -85,9 +85,25 @@ def build_workload(name):
         r = 16.0
         topo = G.straight_pipe(radius=r, length=136, box=(40, 40, 136))
         desc = "straight pipe R=16 lu in a 40x40x136 box"
+    elif name == "aneurysm":
+        r = 20.0
+        topo = G.saccular_aneurysm()
+        desc = "saccular aneurysm: R=20 tube, 90 deg bend of radius 120, R=40 sac, box 1024x512x512"
+    elif name == "bifurcation":
+        r = 24.0
+        topo = G.y_bifurcation()
+        desc = "Y-bifurcation, parent R=24 L=200, daughters R=18/16 at +-35 deg, box 256x256x348 (D3Q27)"
+    elif name == "stenosed":
+        r = 24.0
+        topo = G.straight_pipe(radius=24.0, length=384, box=(64, 64, 384), stenosis=0.6, stenosis_sigma=12.0)
+        desc = "stenosed pipe R=24 lu, 64x64x384 box, 60% radius stenosis"
     else:
         raise SystemExit("unknown workload " + name)
     return topo, desc, r
+
+
+def workload_lattice(name):
+    return 27 if name == "bifurcation" else 19
 
 
 def measured_peaks():
@@ -211,11 +227,11 @@ def replica_mlups(n_nodes, steps, max_ms, world):
     return n_nodes * steps / (max_ms / 1e3) / 1e6 * world
 
 
-def time_engine(topo, storage, steps, warmup, device, torch, vel, bc="physics", radius=None, before=None):
+def time_engine(topo, storage, steps, warmup, device, torch, vel, bc="physics", radius=None, before=None, q=19):
     from lbm_b200 import Engine
     # reference boundaries diverge at tau 0.52 (as the reference itself does);
     # their timing runs on through the non-finite values, as the reference would
-    eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, storage=storage, device=device, bc=bc,
+    eng = Engine(topo, tau=TAU, dt=1e-5, spacing=1.0, lattice=q, storage=storage, device=device, bc=bc,
                  numeric_check=(bc == "physics"))
     eng.set_flow(False, vel)
     if bc == "physics":
@@ -249,7 +265,7 @@ def run_gpu(args):
     n = len(topo["kind"])
     storage = args.storage
     S = BYTES_PER_POP[storage]
-    Q = 19
+    Q = workload_lattice(args.workload)
 
     # headline: K steps on the engine stream, CUDA events, barrier + sync on
     # both sides of the timed region
@@ -260,7 +276,7 @@ def run_gpu(args):
 
     with ClockSampler(device) as clk:
         eng, total_ms, ms_step, ms_bnd = time_engine(topo, storage, args.steps, args.warmup, device, torch, vel,
-                                                     args.bc, radius, before=barrier)
+                                                     args.bc, radius, before=barrier, q=Q)
     barrier()
     total_ms = max_over_ranks(total_ms, dist, "cuda")
     clocks = clk.summary()
@@ -305,6 +321,9 @@ def run_gpu(args):
     voxel = None
     if rank == 0 and not args.no_voxel:
         voxel = run_voxel(torch, device)
+    jt = None
+    if rank == 0 and not args.no_jt:
+        jt = run_jt(torch, device)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -318,7 +337,7 @@ def run_gpu(args):
             "dtype": {"f32": "f32 (storage f - w), f32 compute", "f16": "f16 storage, f32 compute",
                       "bf16": "bf16 storage, f32 compute", "f64": "f64"}[storage],
             "data": "synthetic (analytic vessel geometry, f = w initial state)",
-            "config": {"workload": desc, "lattice": "D3Q19", "fluid_nodes": n,
+            "config": {"workload": desc, "lattice": "D3Q%d" % Q, "fluid_nodes": n,
                        "box_cells": BOX[0] * BOX[1] * BOX[2] if args.workload.startswith("tortuous") else None,
                        "tau": TAU, "inlet_velocity": round(vel, 6), "reynolds": REYNOLDS, "storage": storage,
                        "bc_mode": args.bc, "segments": info["n_segments"],
@@ -328,16 +347,17 @@ def run_gpu(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": 2 * args.steps, "clocks": clocks, "device_flags": flags,
             "variants": variants, "precision": precision, "adjoint": adjoint, "configs": configs, "geometry_setup": voxel,
+            "shipped_case": jt,
         }
         # the key figures once more, last on the line (a reader of its tail
         # sees them)
-        line["summary"] = summary(storage, mlups, roofline, variants, precision, adjoint, configs, cpu)
+        line["summary"] = summary(storage, mlups, roofline, variants, precision, adjoint, configs, cpu, jt)
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
 
 
-def summary(storage, mlups, roofline, variants, precision, adjoint, configs, cpu):
+def summary(storage, mlups, roofline, variants, precision, adjoint, configs, cpu, jt=None):
     """Headline figures of every section, in one small block."""
     def get(d, *keys):
         for k in keys:
@@ -380,6 +400,10 @@ def summary(storage, mlups, roofline, variants, precision, adjoint, configs, cpu
                            "adjoint_cost_vs_forward_step": get(configs, "aneurysm_adjoint",
                                                                "cost_per_step_vs_forward_step")}
         out["bifurcation_f32_MLUPS"] = get(configs, "bifurcation", "f32", "MLUPS")
+    if jt:
+        out["shipped_case_jt"] = {"nodes": jt["nodes"], "gpu_setup_seconds": jt["gpu_setup_seconds"],
+                                  "reference_f64_MLUPS": get(jt, "reference_f64", "MLUPS"),
+                                  "physics_f32_MLUPS": get(jt, "physics_f32", "MLUPS")}
     if cpu:
         out["cpu_reference_MLUPS"] = {"value": cpu.get("value"), "cores": cpu.get("cores"),
                                       "cpu_model": cpu.get("cpu_model")}
@@ -721,6 +745,52 @@ def run_voxel(torch, device):
     return out
 
 
+# ------------------------------------------------------- the shipped case ---
+JT_FIXTURE = os.path.join(ROOT, "tests", "golden", "jt_g0.2.npz")
+JT_GRID = 0.025
+
+
+def run_jt(torch, device, steps=200):
+    """The reference's own case: JT.stl (its triangles, as the reference's
+    reader reads them, and its config.txt opening blocks are kept in the
+    JT test fixture) at the config's grid_size 0.025 (318 x 407 x 500 grid
+    points, 64.7M). GPU voxelisation (wall clock, Python array handling
+    included), then the config's tau 0.68 and constant inflow 0.1 through
+    the engine: FP64 and FP32 storage with the reference's boundaries, FP32
+    and FP16 with physics boundaries. The reference's setup labels every grid
+    point against every facet: 27.7 s for the 136k points of grid_size 0.2
+    on one core, so hours at 0.025; it is not timed here."""
+    from lbm_b200 import Engine
+    from lbm_b200 import geometry as G
+    d = np.load(JT_FIXTURE)
+    tris = d["triangles"]
+    ops = json.loads(str(d["openings"]))
+    tau, vel = 0.68, float(d["cte_vel"][0])
+    G.voxelise_stl(tris, 0.2, ops, device=device)  # warm-up (context, module load)
+    t0 = time.perf_counter()
+    topo, (dims, origin, sp, ms) = G.voxelise_stl(tris, JT_GRID, ops, device=device, info=True)
+    wall = time.perf_counter() - t0
+    n = len(topo["kind"])
+    outs = [len(topo["outlet_%d" % k]) for k in range(4) if "outlet_%d" % k in topo]
+    out = {"workload": "JT.stl with its config.txt, grid_size %g" % JT_GRID, "grid": list(dims),
+           "grid_points": int(np.prod(dims)), "nodes": n, "inlet_nodes": len(topo["inlet"]),
+           "outlet_nodes": outs, "near_wall_nodes": len(topo["nearwall"]), "gpu_setup_seconds": round(wall, 3),
+           "tau": tau, "inlet_velocity": vel, "steps": steps}
+    for storage, bc in (("f64", "reference"), ("f32", "reference"), ("f32", "physics"), ("f16", "physics")):
+        e = Engine(topo, tau=tau, dt=1e-5, spacing=sp, storage=storage, device=device, bc=bc, numeric_check=False)
+        e.set_flow(False, vel)
+        if bc == "physics":
+            nrm = np.asarray(topo["inlet_normal"], float)
+            e.set_inlet_profile(np.tile(-vel * nrm, (len(topo["inlet"]), 1)))
+        e.set_observation(False)
+        e.step(20)
+        ms_step, ms_bnd = e.step_timed(steps)
+        out["%s_%s" % (bc, storage)] = {"MLUPS": round(n * steps / ((ms_step + ms_bnd) / 1e3) / 1e6, 1),
+                                        "device_flags": e.flags()}
+        e.close()
+    return out
+
+
 # ----------------------------------------------------------------- adjoint ---
 ADJ_STEPS, ADJ_K, ADJ_TAU = 3000, 100, 0.6
 
@@ -740,13 +810,15 @@ def adjoint_workload():
     return topo, basis, a, targets
 
 
-def run_adjoint(torch, device, fd=True):
+def run_adjoint(torch, device, fd=True, steps=None, k=None):
     """Adjoint gradient of the throat's time-averaged WSS^2 w.r.t. 8 inlet
     coefficients and tau (3000 steps, checkpoint every 100): FP32 cost per
     step against the engine's FP32 forward step on the same pipe, and
     accuracy against an FP64 adjoint and central differences (h = 1e-4) of
     the FP64 objective."""
     from lbm_b200 import Engine
+    T = steps or ADJ_STEPS
+    K = k or ADJ_K
     topo, basis, a, targets = adjoint_workload()
     n = len(topo["kind"])
 
@@ -759,26 +831,26 @@ def run_adjoint(torch, device, fd=True):
     fw.set_inlet_profile((a @ basis)[:, None] * -np.asarray(topo["inlet_normal"], dtype=np.float64)[None, :])
     fw.set_observation(False)
     fw.step(20)
-    ms_step, ms_bnd = fw.step_timed(ADJ_STEPS)
+    ms_step, ms_bnd = fw.step_timed(T)
     fw.close()
-    fwd_ms = (ms_step + ms_bnd) / ADJ_STEPS
+    fwd_ms = (ms_step + ms_bnd) / T
 
     e = engine(ADJ_TAU)
     e.adjoint(50, targets, basis, a, checkpoint_every=10, precision="f32")   # warm-up
-    r32 = e.adjoint(ADJ_STEPS, targets, basis, a, checkpoint_every=ADJ_K, precision="f32")
-    r64 = e.adjoint(ADJ_STEPS, targets, basis, a, checkpoint_every=ADJ_K, precision="f64")
+    r32 = e.adjoint(T, targets, basis, a, checkpoint_every=K, precision="f32")
+    r64 = e.adjoint(T, targets, basis, a, checkpoint_every=K, precision="f64")
     g32 = np.append(r32["grad_coeffs"], r32["dJ_dtau"])
     g64 = np.append(r64["grad_coeffs"], r64["dJ_dtau"])
     total32 = r32["forward_ms"] + r32["reverse_ms"]
     out = {"workload": "stenosed pipe R=24 lu, 64x64x384 box, 60%% radius stenosis; %d fluid nodes, "
                        "%d throat near-wall nodes" % (n, len(targets)),
-           "steps": ADJ_STEPS, "checkpoint_every": ADJ_K, "tau": ADJ_TAU, "parameters": "8 inlet modes + tau",
+           "steps": T, "checkpoint_every": K, "tau": ADJ_TAU, "parameters": "8 inlet modes + tau",
            "J_f32": r32["J"], "J_f64": r64["J"],
            "engine_forward_step_ms_f32": round(fwd_ms, 5),
            "adjoint_ms_f32": {"forward_sweep": round(r32["forward_ms"], 2),
                               "recompute_and_reverse": round(r32["reverse_ms"], 2)},
            "steps_recomputed": r32["steps_recomputed"],
-           "cost_per_step_vs_forward_step": round(total32 / ADJ_STEPS / fwd_ms, 3),
+           "cost_per_step_vs_forward_step": round(total32 / T / fwd_ms, 3),
            "device_bytes_f32": r32["device_bytes"],
            "grad_f32_vs_f64_rel": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
            "grad_f64": g64.tolist()}
@@ -789,12 +861,12 @@ def run_adjoint(torch, device, fd=True):
             ap, am = a.copy(), a.copy()
             ap[j] += h
             am[j] -= h
-            g_fd[j] = (e.adjoint(ADJ_STEPS, targets, basis, ap, gradient=False, precision="f64")["J"] -
-                       e.adjoint(ADJ_STEPS, targets, basis, am, gradient=False, precision="f64")["J"]) / (2 * h)
+            g_fd[j] = (e.adjoint(T, targets, basis, ap, gradient=False, precision="f64")["J"] -
+                       e.adjoint(T, targets, basis, am, gradient=False, precision="f64")["J"]) / (2 * h)
         jt = []
         for t in (ADJ_TAU + h, ADJ_TAU - h):
             et = engine(t)
-            jt.append(et.adjoint(ADJ_STEPS, targets, basis, a, gradient=False, precision="f64")["J"])
+            jt.append(et.adjoint(T, targets, basis, a, gradient=False, precision="f64")["J"])
             et.close()
         g_fd[8] = (jt[0] - jt[1]) / (2 * h)
         out["fd_h"] = h
@@ -925,7 +997,13 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--no-voxel", action="store_true")
-    ap.add_argument("--section", default="all", choices=["all", "precision", "adjoint", "configs", "voxel"],
+    ap.add_argument("--no-jt", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=None,
+                    help="--section adjoint: steps of the adjoint runs (default 3000)")
+    ap.add_argument("--no-fd", action="store_true", help="--section adjoint: skip the central differences")
+    ap.add_argument("--adjoint-k", type=int, default=None,
+                    help="--section adjoint: checkpoint interval (default 100)")
+    ap.add_argument("--section", default="all", choices=["all", "precision", "adjoint", "configs", "voxel", "jt"],
                     help="run only the precision study, the adjoint measurement or the branching/aneurysm runs")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -936,8 +1014,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         run = {"precision": run_precision, "adjoint": run_adjoint, "configs": run_configs,
-               "voxel": run_voxel}[args.section]
-        res = run(torch, 0)
+               "voxel": run_voxel, "jt": run_jt}[args.section]
+        if args.section == "adjoint":
+            res = run_adjoint(torch, 0, fd=not args.no_fd, steps=args.adjoint_steps, k=args.adjoint_k)
+        else:
+            res = run(torch, 0)
         print(json.dumps({"section": args.section, **res}))
     else:
         run_gpu(args)

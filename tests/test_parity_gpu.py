@@ -25,7 +25,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 SMALL = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-               if not os.path.basename(p).startswith("pipe16"))
+               if not os.path.basename(p).startswith(("pipe16", "jt_")))
 STEPS = {"cyl_z": 60, "cyl_z_rev": 20, "cyl_x": 40, "cyl_x_rev": 20, "cyl_y": 4, "cyl_y_rev": 4,
          "cyl_z_pulsatile": 100, "outlet_chain": 12}
 STABLE = ["cyl_z", "cyl_z_rev", "cyl_x", "cyl_x_rev", "outlet_chain"]

@@ -120,8 +120,11 @@ def measured_peaks():
 # over the two phase kernels of one step, from an ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum on the step kernels (command
 # and case in profiles/step_kernel_traffic_d3q19.md); None where not captured.
-STEP_KERNEL_TRAFFIC = {}
-TRAFFIC_SOURCE = None
+STEP_KERNEL_TRAFFIC = {"f32": 157.6, "f16": 82.07}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one phase-0 and one phase-1 launch "
+                  "on the default workload (21,381,419 nodes, 1.6 GB FP32 state, 13x L2), averaged: FP32 "
+                  "3.35 and 3.39 GB, FP16 1.741 and 1.769 GB per launch; the excess over the algorithmic "
+                  "2 Q S per node is the node words (4 B), segment rows and the near-wall hand-off")
 
 
 def host_cpu():
@@ -290,7 +293,7 @@ def run_gpu(args):
     alg_bytes = 2 * Q * S * n
     step_avg_ms = ms_step / args.steps
     achieved = alg_bytes / (step_avg_ms / 1e3) / 1e9
-    tpn = STEP_KERNEL_TRAFFIC.get(storage)
+    tpn = STEP_KERNEL_TRAFFIC.get(storage) if (args.workload == "tortuous8" and args.bc == "physics") else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": round(tpn * n) if tpn else None,

@@ -218,7 +218,11 @@ int lbm_get_flags(lbm_engine* e, uint32_t* flags);
  * class (milliseconds, summed over the steps, CUDA events on the engine's
  * stream): the stream+collide kernel, and the boundary work around it — the
  * pre-pass (wall shear stress, outlet copy sources) in reference mode, the
- * post-pass (wall shear stress, open-boundary corrections) in physics mode. */
+ * post-pass (wall shear stress, open-boundary corrections) in physics mode.
+ * The events are recorded around a sample of the steps (the two that begin
+ * every 32 steps, one of each phase), and the sums are the sampled averages
+ * times n_steps: an event between every pair of kernels would add about 10 us
+ * of device time to each step. */
 int lbm_step_timed(lbm_engine* e, int64_t n_steps, double* step_kernel_ms, double* boundary_kernel_ms);
 
 /* Sizes: nodes, padded leading dimension, segments, near-wall nodes, outlet

@@ -581,22 +581,35 @@ int observe_bits(const lbm_engine* e, int64_t left) {
     return (left <= 1 ? 2 : 0) | (left == 0 ? 1 : 0);
 }
 
+// Timed runs (lbm_step_timed) record events around sampled steps only: the
+// two steps (one of each phase) that begin every TIMING_STRIDE steps. An
+// event between two kernels of a stream costs the stream about 5 us, which
+// events around every step would add to the very time they measure (1.8 % of
+// a step of the 21.4M-node vessel, 15-28 % on lattices of about a million
+// nodes). The per-class sums are the sampled steps' averages times the
+// step count; each sampled step uses three events.
+constexpr int64_t TIMING_STRIDE = 32;
+bool timing_sample(int64_t i) { return i % TIMING_STRIDE < 2; }
+int64_t timing_samples(int64_t n) { return (n / TIMING_STRIDE) * 2 + std::min<int64_t>(n % TIMING_STRIDE, 2); }
+
 // Physics mode: per step the stream+collide kernel, then one post-pass with
 // that step's wall shear stress and the open-boundary corrections of its
 // store (which streams into the next step). No pre-pass: physics mode has no
-// outlet copy sources. Timed runs record ev[2i] before step kernel i and
-// ev[2i+1] before its post-pass; ev[2n] after the last post-pass. A WSS
-// hand-off left pending by an earlier reference-style sequence is reduced
-// first (never the case in physics mode, where every post-pass reduces it).
+// outlet copy sources. A sampled step of a timed run records events before
+// its step kernel, before its post-pass and after it. A WSS hand-off left
+// pending by an earlier reference-style sequence is reduced first (never the
+// case in physics mode, where every post-pass reduces it).
 int run_steps_physics(lbm_engine* e, int64_t n_steps, int64_t after, double* t_step, double* t_bnd) {
     const bool timed = t_step || t_bnd;
     const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
+    int64_t sample = 0;
     for (int64_t i = 0; i < n_steps; ++i) {
         const int64_t t = e->step + 1;
         const int obs = observe_bits(e, n_steps - 1 - i + after);
         double* mom = e->obs_mom[t % 2];
         const int phase = e->phase;
         const double scale = inlet_factor(e, e->step + 1, pulsatile ? e->runtime + e->dt : e->runtime);
+        cudaEvent_t* ev = timed && timing_sample(i) ? &e->evpool[3 * sample++] : nullptr;
         int rc = dispatch(e, [&](auto tag) {
             using S = typename decltype(tag)::St;
             constexpr int Q = decltype(tag)::q;
@@ -606,12 +619,13 @@ int run_steps_physics(lbm_engine* e, int64_t n_steps, int64_t after, double* t_s
                 if (ce != cudaSuccess) return e->cuda_fail(ce, "wall shear kernel");
                 e->wss_pending = false;
             }
-            if (timed) cudaEventRecord(e->evpool[2 * i], e->stream);
+            if (ev) cudaEventRecord(ev[0], e->stream);
             ce = launch_step<S, Q>(step_args<S, Q>(e, 0.0, mom), phase, e->bc, obs, e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "step kernel");
-            if (timed) cudaEventRecord(e->evpool[2 * i + 1], e->stream);
+            if (ev) cudaEventRecord(ev[1], e->stream);
             ce = launch_post<S, Q>(boundary_args<S, Q>(e, 0.0, e->nw() > 0, false), open_args<S, Q>(e, scale),
                                    e->stream);
+            if (ev) cudaEventRecord(ev[2], e->stream);
             return ce == cudaSuccess ? 0 : e->cuda_fail(ce, "post-step kernel");
         });
         if (rc) return rc;
@@ -622,21 +636,20 @@ int run_steps_physics(lbm_engine* e, int64_t n_steps, int64_t after, double* t_s
         if (pulsatile) e->runtime += e->dt;
         e->fresh = false;
     }
-    if (timed) {
-        cudaEventRecord(e->evpool[2 * n_steps], e->stream);
-        cudaEventRecord(e->evpool[2 * n_steps + 1], e->stream);
-        cudaError_t ce = cudaEventSynchronize(e->evpool[2 * n_steps + 1]);
+    if (timed && sample > 0) {
+        cudaError_t ce = cudaEventSynchronize(e->evpool[3 * sample - 1]);
         if (ce != cudaSuccess) return e->cuda_fail(ce, "timed steps");
         double ms_step = 0, ms_bnd = 0;
-        for (int64_t i = 0; i < n_steps; ++i) {
+        for (int64_t j = 0; j < sample; ++j) {
             float a = 0, b = 0;
-            cudaEventElapsedTime(&a, e->evpool[2 * i], e->evpool[2 * i + 1]);
-            cudaEventElapsedTime(&b, e->evpool[2 * i + 1], e->evpool[2 * i + 2]);
+            cudaEventElapsedTime(&a, e->evpool[3 * j], e->evpool[3 * j + 1]);
+            cudaEventElapsedTime(&b, e->evpool[3 * j + 1], e->evpool[3 * j + 2]);
             ms_step += a;
             ms_bnd += b;
         }
-        if (t_step) *t_step = ms_step;
-        if (t_bnd) *t_bnd = ms_bnd;
+        const double scale = (double)n_steps / (double)sample;
+        if (t_step) *t_step = ms_step * scale;
+        if (t_bnd) *t_bnd = ms_bnd * scale;
     }
     return 0;
 }
@@ -673,13 +686,12 @@ int run_steps_checked(lbm_engine* e, int64_t n_steps, int64_t after, double* t_s
     if (t_step) *t_step = 0;
     if (t_bnd) *t_bnd = 0;
     const bool timed = t_step || t_bnd;
-    // timed runs: events ev[2i] before the boundary pass of step i, ev[2i+1]
-    // before its stream+collide kernel, ev[2n] after the last step, ev[2n+1]
-    // after the last step's wall-shear pass; read once at the end so timing
-    // adds no host round trip between steps
+    // timed runs: three events per sampled step (timing_sample) and two
+    // around the last step's wall-shear pass in reference mode, read once at
+    // the end so timing adds no host round trip between steps
     if (timed) {
-        if (n_steps > (1 << 20)) return e->fail(LBM_ERR_ARGUMENT, "too many timed steps in one call");
-        while ((int64_t)e->evpool.size() < 2 * n_steps + 2) {
+        if (n_steps > (1 << 24)) return e->fail(LBM_ERR_ARGUMENT, "too many timed steps in one call");
+        while ((int64_t)e->evpool.size() < 3 * timing_samples(n_steps) + 2) {
             cudaEvent_t ev;
             cudaError_t ce = cudaEventCreate(&ev);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "event");
@@ -687,6 +699,7 @@ int run_steps_checked(lbm_engine* e, int64_t n_steps, int64_t after, double* t_s
         }
     }
     if (e->bc == LBM_BC_PHYSICS) return run_steps_physics(e, n_steps, after, t_step, t_bnd);
+    int64_t sample = 0;
     for (int64_t i = 0; i < n_steps; ++i) {
         const int64_t t = e->step + 1;
         const bool pulsatile = e->flow == LBM_FLOW_PULSATILE;
@@ -696,16 +709,18 @@ int run_steps_checked(lbm_engine* e, int64_t n_steps, int64_t after, double* t_s
         const int obs = observe_bits(e, n_steps - 1 - i + after);
         double* mom = e->obs_mom[t % 2];
         const int phase = e->phase;
+        cudaEvent_t* ev = timed && timing_sample(i) ? &e->evpool[3 * sample++] : nullptr;
         int rc = dispatch(e, [&](auto tag) {
             using S = typename decltype(tag)::St;
             constexpr int Q = decltype(tag)::q;
-            if (timed) cudaEventRecord(e->evpool[2 * i], e->stream);
+            if (ev) cudaEventRecord(ev[0], e->stream);
             cudaError_t ce =
                 launch_boundary<S, Q>(boundary_args<S, Q>(e, vel, e->wss_pending, true), phase, e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "boundary kernel");
-            if (timed) cudaEventRecord(e->evpool[2 * i + 1], e->stream);
+            if (ev) cudaEventRecord(ev[1], e->stream);
             ce = launch_step<S, Q>(step_args<S, Q>(e, vel, mom), phase, e->bc, obs, e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "step kernel");
+            if (ev) cudaEventRecord(ev[2], e->stream);
             return 0;
         });
         if (rc) return rc;
@@ -720,7 +735,8 @@ int run_steps_checked(lbm_engine* e, int64_t n_steps, int64_t after, double* t_s
         e->fresh = false;
     }
     // wall shear stress of the last step
-    if (timed) cudaEventRecord(e->evpool[2 * n_steps], e->stream);
+    cudaEvent_t* last_ev = timed ? &e->evpool[3 * sample] : nullptr;
+    if (last_ev) cudaEventRecord(last_ev[0], e->stream);
     if (e->wss_pending) {
         int rc = dispatch(e, [&](auto tag) {
             using S = typename decltype(tag)::St;
@@ -732,19 +748,22 @@ int run_steps_checked(lbm_engine* e, int64_t n_steps, int64_t after, double* t_s
         e->wss_pending = false;
     }
     if (timed) {
-        cudaEventRecord(e->evpool[2 * n_steps + 1], e->stream);
-        cudaError_t ce = cudaEventSynchronize(e->evpool[2 * n_steps + 1]);
+        cudaEventRecord(last_ev[1], e->stream);
+        cudaError_t ce = cudaEventSynchronize(last_ev[1]);
         if (ce != cudaSuccess) return e->cuda_fail(ce, "timed steps");
         double ms_step = 0, ms_bnd = 0;
-        for (int64_t i = 0; i < n_steps; ++i) {
+        for (int64_t j = 0; j < sample; ++j) {
             float a = 0, b = 0;
-            cudaEventElapsedTime(&a, e->evpool[2 * i], e->evpool[2 * i + 1]);
-            cudaEventElapsedTime(&b, e->evpool[2 * i + 1], e->evpool[2 * i + 2]);
+            cudaEventElapsedTime(&a, e->evpool[3 * j], e->evpool[3 * j + 1]);
+            cudaEventElapsedTime(&b, e->evpool[3 * j + 1], e->evpool[3 * j + 2]);
             ms_bnd += a;
             ms_step += b;
         }
+        const double scale = sample > 0 ? (double)n_steps / (double)sample : 0.0;
+        ms_step *= scale;
+        ms_bnd *= scale;
         float last = 0;
-        cudaEventElapsedTime(&last, e->evpool[2 * n_steps], e->evpool[2 * n_steps + 1]);
+        cudaEventElapsedTime(&last, last_ev[0], last_ev[1]);
         ms_bnd += last;
         if (t_step) *t_step = ms_step;
         if (t_bnd) *t_bnd = ms_bnd;

@@ -685,13 +685,23 @@ __device__ __forceinline__ void open_item(const OpenArgs<S, Q>& a, int i) {
             uv[c] = a.io_u[3 * (long long)k + c];
         }
     }
+    // every corrected slot is read before any is written: the loads go out
+    // together instead of one memory round trip per link
+    C f_all[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        f_all[q] = C(0);
+        if (q == L::REST || ((m >> q) & 1)) continue;
+        const double cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
+        if (cn > 0.0) f_all[q] = Store<S>::get(a.pop + (long long)L::opp(q) * a.ld + n);
+    }
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         if (q == L::REST || ((m >> q) & 1)) continue;
         const double cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
         if (!(cn > 0.0)) continue;
         S* slot = a.pop + (long long)L::opp(q) * a.ld + n;
-        const double f = (double)Store<S>::get(slot);
+        const double f = (double)f_all[q];
         const double cu = L::cx(q) * uv[0] + L::cy(q) * uv[1] + L::cz(q) * uv[2];
         double v;
         if (inlet) {
@@ -756,20 +766,22 @@ __global__ void boundary_kernel(BoundaryArgs<S, Q> a) {
     a.out_buf[(long long)k * Q + q] = Store<S>::get(a.pop + idx);
 }
 
-// Physics-mode pass after each step kernel: the wall shear stress of the
-// step just taken (items [0, n_wss)) and the open-boundary corrections of its
-// store (then one item per inlet / outlet node). The two touch disjoint data
-// (the near-wall hand-off buffers and accumulators; the inlet and outlet
-// nodes' bounce-back slots), so one launch does both.
+// Physics-mode pass after each step kernel: the open-boundary corrections of
+// its store (items [0, n_in + n_out): one per inlet / outlet node) and the
+// wall shear stress of the step just taken (then one item per near-wall
+// node). The two touch disjoint data (the inlet and outlet nodes' bounce-back
+// slots; the near-wall hand-off buffers and accumulators), so one launch does
+// both; the open-boundary items, the longer ones, go first so that they do not
+// trail the launch.
 template <class S, int Q>
 __global__ void post_kernel(BoundaryArgs<S, Q> b, OpenArgs<S, Q> o) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < b.n_wss) {
-        wall_shear<S, Q>(b, (int)i);
+    const long long n_open = (long long)o.n_in + o.n_out;
+    if (i < n_open) {
+        open_item<S, Q>(o, (int)i);
         return;
     }
-    const long long j = i - b.n_wss;
-    if (j < (long long)o.n_in + o.n_out) open_item<S, Q>(o, (int)j);
+    if (i - n_open < b.n_wss) wall_shear<S, Q>(b, (int)(i - n_open));
 }
 
 }  // namespace lbm

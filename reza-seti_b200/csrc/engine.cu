@@ -906,7 +906,8 @@ int create(const lbm_desc* d, lbm_engine** out) {
     if ((ce = e->alloc(&nwm, (size_t)4 * std::max(1, e->nw()) * celem)) != cudaSuccess) return bail(ce, "near-wall");
     e->nw_mom = nwm;
     char* nws = nullptr;
-    if ((ce = e->alloc(&nws, (size_t)e->Q * std::max(1, e->nw()) * celem)) != cudaSuccess) return bail(ce, "near-wall");
+    const size_t rows = celem == 8 ? (size_t)e->Q : (size_t)lbm::handoff_rows<float, 19>();
+    if ((ce = e->alloc(&nws, rows * std::max(1, e->nw()) * celem)) != cudaSuccess) return bail(ce, "near-wall");
     e->nw_s = nws;
     if ((ce = e->alloc(&e->wss, (size_t)e->nw())) != cudaSuccess) return bail(ce, "wss");
     if ((ce = e->alloc(&e->acc, (size_t)3 * e->nw())) != cudaSuccess) return bail(ce, "wss");

@@ -103,8 +103,10 @@ struct StepArgs {
     // physics mode: velocity of each outlet node's collision, [n_out][3],
     // for the open-boundary pass
     double* io_u;
-    // near-wall nodes: their arriving populations, [Q][n_nw], for the wall
-    // shear stress computed by the next boundary pass (aux[n] is the index)
+    // near-wall nodes hand the wall-shear pass what it needs of the step,
+    // [handoff_rows][n_nw] (aux[n] is the index): FP64 the Q arriving
+    // populations, the shifted types their six second moments and the
+    // collision's drho, u
     C* nw_s;
     int n_nw;
     // observation (written only by observing launches)
@@ -129,7 +131,7 @@ struct BoundaryArgs {
     // when there is none pending)
     int n_wss;
     int n_nw;
-    const C* nw_s;            // [Q][n_nw] arriving populations of the previous step
+    const C* nw_s;            // [handoff_rows][n_nw] hand-off of the previous step
     // normals and moments in the compute type: the FP32 traction reads both
     // as float, and the moments it stores are FP32 values, so FP32 storage
     // keeps them exactly in 28 instead of 56 bytes per node
@@ -383,6 +385,49 @@ __device__ __forceinline__ void wall_fixup(C s[Q], typename Meta<Q>::T m) {
 }
 
 // ------------------------------------------------------ wall shear stress ---
+// Rows of the near-wall hand-off per node. FP64 hands over the Q arriving
+// populations: the reference's triple loop runs on f - f_eq per direction.
+// The shifted types hand over what their traction needs, 10 values instead
+// of Q: the second moments Pi_ab = sum_q d_q c_qa c_qb of the arriving
+// deviations (rows 0-5: xx yy zz xy xz yz) and the moments of the node's
+// collision, drho and u (rows 6-9), which become the f_eq of the next step's
+// wall shear stress.
+template <class C, int Q>
+__host__ __device__ constexpr int handoff_rows() {
+    return sizeof(C) == 8 ? Q : 10;
+}
+constexpr int HANDOFF_MOM_ROW = 6;
+
+// Pi_ab = sum_q v_q c_qa c_qb over the moving directions, entry J of
+// xx yy zz xy xz yz, for a scalar or a packed pair (add / sub give the
+// arithmetic). One entry at a time: a caller that stores each entry as it
+// comes holds one accumulator, not six.
+template <int Q, int J, class T, class Add, class Sub>
+__device__ __forceinline__ T second_moment(const T v[Q], T zero, Add add, Sub sub) {
+    using L = Lat<Q>;
+    constexpr int A = J < 3 ? J : (J == 5 ? 1 : 0);  // the entry's two axes
+    constexpr int B = J < 3 ? J : (J == 3 ? 1 : 2);
+    T p = zero;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int c[3] = {L::cx(q), L::cy(q), L::cz(q)};
+        const int cc = c[A] * c[B];
+        if (cc > 0) p = add(p, v[q]);
+        else if (cc < 0) p = sub(p, v[q]);
+    }
+    return p;
+}
+
+template <int Q, class T, class Add, class Sub>
+__device__ __forceinline__ void second_moments(const T v[Q], T P[6], T zero, Add add, Sub sub) {
+    P[0] = second_moment<Q, 0>(v, zero, add, sub);
+    P[1] = second_moment<Q, 1>(v, zero, add, sub);
+    P[2] = second_moment<Q, 2>(v, zero, add, sub);
+    P[3] = second_moment<Q, 3>(v, zero, add, sub);
+    P[4] = second_moment<Q, 4>(v, zero, add, sub);
+    P[5] = second_moment<Q, 5>(v, zero, add, sub);
+}
+
 // Simulation::ComputeWallShearStress (Simulation.cpp:767-799), operand order
 // kept. fne[q] = f - f_eq of the near-wall node.
 template <class C, int Q>
@@ -408,16 +453,17 @@ __device__ __forceinline__ void shear_traction(const C fne[Q], const double nrm_
     }
 }
 
-// Wall shear stress of near-wall node k from its arriving populations s and
+// Wall shear stress of near-wall node k from what its step handed over and
 // the moments its previous collision used (the f_eq the reference keeps in
 // m_eqdistributions), accumulated in FP64 (Simulation.cpp:767-799).
 template <class S, int Q>
 __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
     using C = typename Store<S>::C;
     using L = Lat<Q>;
-    C s[Q];
+    constexpr int R = handoff_rows<C, Q>();
+    C h[R];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) s[q] = a.nw_s[(long long)q * a.n_nw + k];
+    for (int r = 0; r < R; ++r) h[r] = a.nw_s[(long long)r * a.n_nw + k];
     C* mom = a.nw_mom + 4 * (long long)k;
     const C* nd = a.nw_normal + 3 * (long long)k;
     // the accumulators are read with the rest, not after the stores below:
@@ -425,32 +471,33 @@ __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
     double* acc = a.acc + 3 * (long long)k;
     const double acc0 = acc[0], acc1 = acc[1], acc2 = acc[2], accm = a.accmag[k];
     double tau[3];
+    C m0, u[3];
     if constexpr (sizeof(C) == 8) {
         // FP64: the reference's own triple loop, operand order kept
         C fne[Q];
-        const double u[3] = {mom[1], mom[2], mom[3]};
+        const double up[3] = {mom[1], mom[2], mom[3]};
 #pragma unroll
-        for (int q = 0; q < Q; ++q) fne[q] = s[q] - feq_ref<Q>(q, mom[0], u);
+        for (int q = 0; q < Q; ++q) fne[q] = h[q] - feq_ref<Q>(q, mom[0], up);
         shear_traction<C, Q>(fne, nd, a.wss_c, tau);
+        // moments of these populations: the f_eq of the next step's WSS (the
+        // same arithmetic as that step's collision of this node)
+        double rho;
+        moments_ref<Q>(h, false, rho, u);
+        m0 = rho;
     } else {
-        // FP32: the same traction through the non-equilibrium stress tensor,
+        // the traction through the non-equilibrium stress tensor,
         // Pi_ab = sum_q fne_q c_qa c_qb:  sum_q fne_q (c.n)(c_a - (c.n) n_a)
-        // = (Pi n)_a - (n.Pi.n) n_a
-        const float u[3] = {(float)mom[1], (float)mom[2], (float)mom[3]};
+        // = (Pi n)_a - (n.Pi.n) n_a, with Pi(fne) = Pi(d) - Pi(deq)
+        const float up[3] = {(float)mom[1], (float)mom[2], (float)mom[3]};
         const float drho = (float)mom[0];
-        float P[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // xx yy zz xy xz yz
+        float de[Q], Pe[6];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            if (q == L::REST) continue;
-            const float fne = s[q] - deq_shifted<Q>(q, drho, u);
-            const int x = L::cx(q), y = L::cy(q), z = L::cz(q);
-            if (x) P[0] += fne;
-            if (y) P[1] += fne;
-            if (z) P[2] += fne;
-            if (x && y) P[3] += x * y > 0 ? fne : -fne;
-            if (x && z) P[4] += x * z > 0 ? fne : -fne;
-            if (y && z) P[5] += y * z > 0 ? fne : -fne;
-        }
+        for (int q = 0; q < Q; ++q) de[q] = q == L::REST ? 0.f : deq_shifted<Q>(q, drho, up);
+        second_moments<Q>(de, Pe, 0.f, [](float x, float y) { return x + y; },
+                          [](float x, float y) { return x - y; });
+        float P[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) P[j] = h[j] - Pe[j];
         const float n0 = (float)nd[0], n1 = (float)nd[1], n2 = (float)nd[2];
         const float pn0 = P[0] * n0 + P[3] * n1 + P[4] * n2;
         const float pn1 = P[3] * n0 + P[1] * n1 + P[5] * n2;
@@ -459,6 +506,11 @@ __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
         tau[0] = a.wss_c * (double)(pn0 - t * n0);
         tau[1] = a.wss_c * (double)(pn1 - t * n1);
         tau[2] = a.wss_c * (double)(pn2 - t * n2);
+        // the moments this step's collision used, handed over by the step
+        m0 = h[HANDOFF_MOM_ROW];
+        u[0] = h[HANDOFF_MOM_ROW + 1];
+        u[1] = h[HANDOFF_MOM_ROW + 2];
+        u[2] = h[HANDOFF_MOM_ROW + 3];
     }
     const double w = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
     a.wss[k] = w;
@@ -466,16 +518,6 @@ __device__ __forceinline__ void wall_shear(const BoundaryArgs<S, Q>& a, int k) {
     acc[1] = acc1 + tau[1];
     acc[2] = acc2 + tau[2];
     a.accmag[k] = accm + w;
-    // moments of these populations: the f_eq of the next step's WSS (the
-    // same arithmetic as that step's collision of this node)
-    C m0, u[3];
-    if constexpr (sizeof(C) == 8) {
-        double rho;
-        moments_ref<Q>(s, false, rho, u);
-        m0 = rho;
-    } else {
-        moments_shifted<Q>(s, false, m0, u);
-    }
     mom[0] = m0;
     mom[1] = u[0];
     mom[2] = u[1];
@@ -540,17 +582,37 @@ __global__ void __launch_bounds__(BLOCK_NODES, Store<S>::MIN_BLOCKS) step_kernel
             a.obs_pop[(long long)q * a.ld + n] = Store<S>::SHIFTED ? (double)s[q] + L::w(q) : (double)s[q];
     }
 
-    // near-wall nodes hand their arriving populations to the boundary pass
-    // that computes this step's wall shear stress
-    if ((m >> Meta<Q>::NW_SHIFT) & 1) {
+    // near-wall nodes hand the boundary pass that computes this step's wall
+    // shear stress their arriving populations (FP64) or their second moments
+    // and, after the collision, its moments (the shifted types)
+    const bool nw = (m >> Meta<Q>::NW_SHIFT) & 1;
+    if (nw) {
         const int k = a.aux[n];
+        if constexpr (sizeof(C) == 8) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) a.nw_s[(long long)q * a.n_nw + k] = s[q];
+            for (int q = 0; q < Q; ++q) a.nw_s[(long long)q * a.n_nw + k] = s[q];
+        } else {
+            float P[6];
+            second_moments<Q>(s, P, 0.f, [](float x, float y) { return x + y; },
+                              [](float x, float y) { return x - y; });
+#pragma unroll
+            for (int j = 0; j < 6; ++j) a.nw_s[(long long)j * a.n_nw + k] = P[j];
+        }
     }
 
     C c[Q], m0, u[3];
     collide<C, Q>(s, BC == BC_REFERENCE && kind == KIND_WALL, a.omega, c, m0, u);
     if (!isfinite((double)m0)) atomicOr(a.flags, FLAG_NONFINITE);
+    if constexpr (sizeof(C) != 8) {
+        // a near-wall node is never a wall node: u is its velocity
+        if (nw) {
+            C* h = a.nw_s + (long long)HANDOFF_MOM_ROW * a.n_nw + a.aux[n];
+            h[0] = m0;
+            h[a.n_nw] = u[0];
+            h[2 * (long long)a.n_nw] = u[1];
+            h[3 * (long long)a.n_nw] = u[2];
+        }
+    }
 
     if (OBS & 2) {
         a.obs_mom[n] = Store<S>::SHIFTED ? 1.0 + (double)m0 : (double)m0;

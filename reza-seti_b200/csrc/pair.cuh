@@ -151,19 +151,42 @@ __device__ __forceinline__ void pair_middle(const StepArgs<S, Q>& a, float2 s[Q]
             if (live1) a.obs_pop[(long long)q * a.ld + n1] = (double)s[q].y + L::w(q);
         }
     }
-    if ((m0 >> Meta<Q>::NW_SHIFT) & 1) {
-        const int k = a.aux[n0];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) a.nw_s[(long long)q * a.n_nw + k] = s[q].x;
-    }
-    if ((m1 >> Meta<Q>::NW_SHIFT) & 1) {
-        const int k = a.aux[n1];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) a.nw_s[(long long)q * a.n_nw + k] = s[q].y;
+    // near-wall nodes hand the wall-shear pass the second moments of their
+    // arriving deviations and, after the collision, its moments
+    const bool nw0 = (m0 >> Meta<Q>::NW_SHIFT) & 1, nw1 = (m1 >> Meta<Q>::NW_SHIFT) & 1;
+    if (nw0 || nw1) {
+        float* h0 = a.nw_s + (nw0 ? a.aux[n0] : 0);
+        float* h1 = a.nw_s + (nw1 ? a.aux[n1] : 0);
+        auto add = [](float2 x, float2 y) { return f2add(x, y); };
+        auto sub = [](float2 x, float2 y) { return f2sub(x, y); };
+        auto put = [&](int j, float2 p) {
+            if (nw0) h0[(long long)j * a.n_nw] = p.x;
+            if (nw1) h1[(long long)j * a.n_nw] = p.y;
+        };
+        put(0, second_moment<Q, 0>(s, f2s(0.f), add, sub));
+        put(1, second_moment<Q, 1>(s, f2s(0.f), add, sub));
+        put(2, second_moment<Q, 2>(s, f2s(0.f), add, sub));
+        put(3, second_moment<Q, 3>(s, f2s(0.f), add, sub));
+        put(4, second_moment<Q, 4>(s, f2s(0.f), add, sub));
+        put(5, second_moment<Q, 5>(s, f2s(0.f), add, sub));
     }
     float2 drho, u[3];
     collide_pair<Q>(s, (float)a.omega, drho, u);
     if (!isfinite(drho.x) || (live1 && !isfinite(drho.y))) atomicOr(a.flags, FLAG_NONFINITE);
+    if (nw0) {
+        float* h = a.nw_s + (long long)HANDOFF_MOM_ROW * a.n_nw + a.aux[n0];
+        h[0] = drho.x;
+        h[a.n_nw] = u[0].x;
+        h[2 * (long long)a.n_nw] = u[1].x;
+        h[3 * (long long)a.n_nw] = u[2].x;
+    }
+    if (nw1) {
+        float* h = a.nw_s + (long long)HANDOFF_MOM_ROW * a.n_nw + a.aux[n1];
+        h[0] = drho.y;
+        h[a.n_nw] = u[0].y;
+        h[2 * (long long)a.n_nw] = u[1].y;
+        h[3 * (long long)a.n_nw] = u[2].y;
+    }
     if (OBS & 2) {
         a.obs_mom[n0] = 1.0 + (double)drho.x;
         a.obs_mom[a.ld + n0] = (double)u[0].x;

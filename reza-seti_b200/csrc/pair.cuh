@@ -83,6 +83,11 @@ constexpr int pair0_min_blocks() {
 // BGK collision of two nodes' deviations d (in place): c = (1 - omega) d +
 // omega deq, deq_q = w_q (drho + (1 + drho)(3 c.u + 4.5 (c.u)^2 - 1.5 u^2)).
 // Returns drho and u of the input.
+//
+// omega w_q deq_q = B_w + t (4.5 c.u + 3) with B_w = omega w (drho - 1.5 rho
+// u^2) and t = omega w rho c.u; the opposite direction has c.u negated, which
+// is B_w + t (4.5 c.u - 3). A direction pair costs c.u, t, two fmas for the
+// brackets, two for the equilibria and two for the relaxations.
 template <int Q>
 __device__ __forceinline__ void collide_pair(float2 d[Q], float omega, float2& drho, float2 u[3]) {
     using L = Lat<Q>;
@@ -98,20 +103,19 @@ __device__ __forceinline__ void collide_pair(float2 d[Q], float omega, float2& d
     }
     drho = f2add(ra, rb);
     const float2 rho = f2add(f2s(1.f), drho);
-    const float2 inv = make_float2(1.f / rho.x, 1.f / rho.y);
+    const float2 inv = make_float2(__frcp_rn(rho.x), __frcp_rn(rho.y));
     u[0] = f2mul(j0, inv);
     u[1] = f2mul(j1, inv);
     u[2] = f2mul(j2, inv);
     const float2 usq = f2fma(u[0], u[0], f2fma(u[1], u[1], f2mul(u[2], u[2])));
-    // deq_q = w (base + rho 4.5 (c.u)^2 + 3 rho c.u), base = drho - 1.5 rho u^2
-    const float2 base = f2fma(rho, f2mul(f2s(-1.5f), usq), drho);
-    const float2 rho3 = f2mul(f2s(3.f), rho);
+    const float2 base = f2fma(rho, f2mul(f2s(-1.5f), usq), drho);  // drho - 1.5 rho u^2
     const float2 keep = f2s(1.f - omega);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const int o = L::opp(q);
+        const float ow = omega * (float)L::w(q);
         if (q == L::REST) {
-            d[q] = f2fma(keep, d[q], f2mul(f2s(omega * (float)L::w(q)), base));
+            d[q] = f2fma(keep, d[q], f2mul(f2s(ow), base));
             continue;
         }
         if (o < q) continue;  // handled with its opposite
@@ -129,11 +133,13 @@ __device__ __forceinline__ void collide_pair(float2 d[Q], float omega, float2& d
         acc(L::cx(q), u[0]);
         acc(L::cy(q), u[1]);
         acc(L::cz(q), u[2]);
-        const float2 sym = f2fma(rho, f2mul(f2mul(f2s(4.5f), cu), cu), base);
-        const float2 anti = f2mul(rho3, cu);
-        const float2 wo = f2s(omega * (float)L::w(q));
-        d[q] = f2fma(keep, d[q], f2mul(wo, f2add(sym, anti)));
-        d[o] = f2fma(keep, d[o], f2mul(wo, f2sub(sym, anti)));
+        // per weight class (the compiler keeps one copy of each)
+        const float2 Bw = f2mul(f2s(ow), base);
+        const float2 t = f2mul(f2mul(f2s(ow), rho), cu);
+        const float2 plus = f2fma(t, f2fma(f2s(4.5f), cu, f2s(3.f)), Bw);
+        const float2 minus = f2fma(t, f2fma(f2s(4.5f), cu, f2s(-3.f)), Bw);
+        d[q] = f2fma(keep, d[q], plus);
+        d[o] = f2fma(keep, d[o], minus);
     }
 }
 

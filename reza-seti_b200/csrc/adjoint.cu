@@ -700,6 +700,17 @@ __device__ __forceinline__ void push_scatter_node(const AGeom<float, Q>& g, floa
     using L = Lat<Q>;
     const unsigned ld = (unsigned)g.ld, un = (unsigned)n;
     const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    if (kind != KIND_INLET && kind != KIND_OUTLET) {
+        // no open link: each value to its neighbour's slot or bounced back
+        // into the node's own opposite slot, no branch between the stores
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const unsigned i = q == L::REST ? q * ld + un
+                                            : (((m >> q) & 1) ? q * ld + (unsigned)(n + sd[q]) : L::opp(q) * ld + un);
+            Dn[i] = c[q];
+        }
+        return;
+    }
     float nrm[3] = {0.f, 0.f, 0.f};
     float vin = 0.f;
     if (kind == KIND_INLET) {
@@ -801,42 +812,169 @@ __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
     }
 }
 
-// One node's pull gather (scalar rules): mu_q, the inlet-speed sensitivity
-// factor and the set of outlet links.
+// The boundary rules of one node's pulled values (scalar rules): mu holds
+// the raw values (lambda^{t+1} of the neighbour along each link, or of the
+// node's own opposite slot where the link is missing) and becomes mu_q; gin
+// gathers the inlet-speed sensitivity factor and out_links the outlet links.
 template <int Q>
-__device__ __forceinline__ void pull_gather_node(const AGeom<float, Q>& g, const float* __restrict__ Ln, int n,
-                                                 typename Meta<Q>::T m, const int* sd, float mu[Q], float& gin,
-                                                 unsigned& out_links) {
+__device__ __forceinline__ void pull_fix_node(const AGeom<float, Q>& g, int n, typename Meta<Q>::T m, float mu[Q],
+                                              float& gin, unsigned& out_links) {
     using L = Lat<Q>;
-    const unsigned ld = (unsigned)g.ld, un = (unsigned)n;
     const int kind = (int)((m >> Meta<Q>::KIND_SHIFT) & 3);
+    if (kind != KIND_INLET && kind != KIND_OUTLET) return;
     float nrm[3] = {0.f, 0.f, 0.f};
     if (kind == KIND_INLET) {
         for (int k = 0; k < 3; ++k) nrm[k] = (float)g.in_normal[k];
-    } else if (kind == KIND_OUTLET) {
+    } else {
         for (int k = 0; k < 3; ++k) nrm[k] = g.out_nrm[3 * (long long)g.aux[n] + k];
     }
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-        float v;
-        if (q == L::REST) {
-            v = Ln[q * ld + un];
-        } else if ((m >> q) & 1) {
-            v = Ln[q * ld + (unsigned)(n + sd[q])];
-        } else {
-            v = Ln[L::opp(q) * ld + un];
-            const float cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
-            if (cn > 0.f) {
-                if (kind == KIND_INLET) {
-                    gin += v * (float)(6.0 * L::w(q)) * cn;
-                } else {
-                    v = -v;
-                    out_links |= 1u << q;
-                }
+        if (q == L::REST || ((m >> q) & 1)) continue;
+        const float cn = L::cx(q) * nrm[0] + L::cy(q) * nrm[1] + L::cz(q) * nrm[2];
+        if (cn > 0.f) {
+            if (kind == KIND_INLET) {
+                gin += mu[q] * (float)(6.0 * L::w(q)) * cn;
+            } else {
+                mu[q] = -mu[q];
+                out_links |= 1u << q;
             }
         }
-        mu[q] = v;
     }
+}
+
+// Slot of lambda^{t+1} that node n pulls in direction q: the neighbour's
+// along the link, or the node's own opposite slot where the link is missing.
+template <int Q>
+__device__ __forceinline__ unsigned pull_slot(unsigned ld, int n, typename Meta<Q>::T m, const int* sd, int q) {
+    using L = Lat<Q>;
+    if (q == L::REST) return q * ld + (unsigned)n;
+    return ((m >> q) & 1) ? q * ld + (unsigned)(n + sd[q]) : L::opp(q) * ld + (unsigned)n;
+}
+
+// One node's pull gather: mu_q, the inlet-speed factor and the outlet links.
+template <int Q>
+__device__ __forceinline__ void pull_gather_node(const AGeom<float, Q>& g, const float* __restrict__ Ln, int n,
+                                                 typename Meta<Q>::T m, const int* sd, float mu[Q], float& gin,
+                                                 unsigned& out_links) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) mu[q] = Ln[pull_slot<Q>((unsigned)g.ld, n, m, sd, q)];
+    pull_fix_node<Q>(g, n, m, mu, gin, out_links);
+}
+
+// A second read of two adjacent floats the thread has just read (an L1 hit).
+__device__ __forceinline__ float2 reload2(const float* p) {
+    float2 v;
+    asm volatile("ld.global.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+}
+
+// The reverse step of a pair once its pulled values mu (boundary rules
+// applied) and the moment sums of f^t (ra + rb = drho, j) and sum mu d are
+// known: lambda^t = (1 - omega) mu + omega (A + B.c) + G terms, stored, plus
+// the objective's term at targets and the inlet-speed sensitivity. Returns
+// the pair's share of dJ/domega.
+template <int Q>
+__device__ __forceinline__ double pull_pair_math(const AGeom<float, Q>& g, float* __restrict__ Lc, double s_t,
+                                                 double* __restrict__ dspeed, const float* __restrict__ Gadd,
+                                                 int n0, bool live1, typename Meta<Q>::T m0,
+                                                 typename Meta<Q>::T m1, const float2 mu[Q], float2 ra, float2 rb,
+                                                 float2 j0, float2 j1, float2 j2, float2 mud, float gin0,
+                                                 float gin1, unsigned ol0, unsigned ol1) {
+    using L = Lat<Q>;
+    const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
+    const float2 drho = f2add(ra, rb);
+    const float2 rho = f2add(f2s(1.f), drho);
+    const float2 irho = make_float2(1.f / rho.x, 1.f / rho.y);
+    const float2 u[3] = {f2mul(j0, irho), f2mul(j1, irho), f2mul(j2, irho)};
+    const float2 usq = f2fma(u[0], u[0], f2fma(u[1], u[1], f2mul(u[2], u[2])));
+    // outlet links: d/du of 2 w rho_out eq(u), times lambda = -mu (scalar, rare)
+    float2 G[3] = {f2s(0.f), f2s(0.f), f2s(0.f)};
+    if (ol0 | ol1) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float c0 = (float)L::cx(q), c1 = (float)L::cy(q), c2 = (float)L::cz(q);
+            const float k2 = (float)(2.0 * L::w(q) * g.out_rho);
+            if ((ol0 >> q) & 1) {
+                const float cu = c0 * u[0].x + c1 * u[1].x + c2 * u[2].x;
+                const float k = -mu[q].x * k2;
+                G[0].x += k * (9.f * cu * c0 - 3.f * u[0].x);
+                G[1].x += k * (9.f * cu * c1 - 3.f * u[1].x);
+                G[2].x += k * (9.f * cu * c2 - 3.f * u[2].x);
+            }
+            if ((ol1 >> q) & 1) {
+                const float cu = c0 * u[0].y + c1 * u[1].y + c2 * u[2].y;
+                const float k = -mu[q].y * k2;
+                G[0].y += k * (9.f * cu * c0 - 3.f * u[0].y);
+                G[1].y += k * (9.f * cu * c1 - 3.f * u[1].y);
+                G[2].y += k * (9.f * cu * c2 - 3.f * u[2].y);
+            }
+        }
+    }
+    // A = sum mu w (1 - 4.5 cu^2 + 1.5 u^2), B = sum mu w (3 + 9 cu) c - 3 u sum mu w,
+    // sum mu deq, over direction pairs (q, opp q): cu flips sign
+    const float2 base = f2fma(rho, f2mul(f2s(-1.5f), usq), drho);
+    const float2 rho3 = f2mul(f2s(3.f), rho);
+    const float2 a0 = f2fma(f2s(1.5f), usq, f2s(1.f));
+    float2 A = f2s(0.f), Wm = f2s(0.f), mueq = f2s(0.f);
+    float2 Bc[3] = {f2s(0.f), f2s(0.f), f2s(0.f)};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int o = L::opp(q);
+        const float2 w = f2s((float)L::w(q));
+        if (q == L::REST) {
+            const float2 wm = f2mul(w, mu[q]);
+            A = f2fma(wm, a0, A);
+            Wm = f2add(Wm, wm);
+            mueq = f2fma(wm, base, mueq);
+            continue;
+        }
+        if (o < q) continue;
+        const float2 cu = cdot2<Q>(q, u);
+        const float2 mp = f2mul(w, f2add(mu[q], mu[o]));
+        const float2 mm = f2mul(w, f2sub(mu[q], mu[o]));
+        const float2 cu2 = f2mul(cu, cu);
+        A = f2fma(mp, f2fma(f2s(-4.5f), cu2, a0), A);
+        Wm = f2add(Wm, mp);
+        const float2 sym = f2fma(rho, f2mul(f2s(4.5f), cu2), base);
+        const float2 anti = f2mul(rho3, cu);
+        mueq = f2fma(sym, mp, f2fma(anti, mm, mueq));
+        // (3 mm + 9 cu mp) c
+        const float2 bk = f2fma(f2s(9.f), f2mul(cu, mp), f2mul(f2s(3.f), mm));
+        if (L::cx(q)) Bc[0] = L::cx(q) > 0 ? f2add(Bc[0], bk) : f2sub(Bc[0], bk);
+        if (L::cy(q)) Bc[1] = L::cy(q) > 0 ? f2add(Bc[1], bk) : f2sub(Bc[1], bk);
+        if (L::cz(q)) Bc[2] = L::cz(q) > 0 ? f2add(Bc[2], bk) : f2sub(Bc[2], bk);
+    }
+    const float2 B[3] = {f2fma(f2s(-3.f), f2mul(u[0], Wm), Bc[0]), f2fma(f2s(-3.f), f2mul(u[1], Wm), Bc[1]),
+                         f2fma(f2s(-3.f), f2mul(u[2], Wm), Bc[2])};
+    const float2 gu = f2fma(G[0], u[0], f2fma(G[1], u[1], f2mul(G[2], u[2])));
+    const float2 keep = f2s(1.f - g.omega), om = f2s(g.omega);
+    // lambda_q = (1 - omega) mu_q + omega (A + B.c_q) + (G.c_q - G.u) / rho
+    const float2 Ao = f2mul(om, A);
+    const float2 ngu = f2mul(f2s(-1.f), f2mul(gu, irho));
+    // targets among the two nodes (near-wall nodes are plain fluid nodes,
+    // aux = their near-wall entry)
+    int tk0 = -1, tk1 = -1;
+    if (Gadd) {
+        if ((m0 >> Meta<Q>::NW_SHIFT) & 1) tk0 = g.nw_target[g.aux[n0]];
+        if (live1 && ((m1 >> Meta<Q>::NW_SHIFT) & 1)) tk1 = g.nw_target[g.aux[n0 + 1]];
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const float2 bc = cdot2<Q>(q, B);
+        const float2 gc = cdot2<Q>(q, G);
+        float2 lam = f2fma(keep, mu[q], f2fma(om, bc, Ao));
+        lam = f2add(lam, f2fma(gc, irho, ngu));
+        if (tk0 >= 0) lam.x += Gadd[(long long)tk0 * Q + q];
+        if (tk1 >= 0) lam.y += Gadd[(long long)tk1 * Q + q];
+        *reinterpret_cast<float2*>(Lc + (q * ld + u0)) = lam;
+    }
+    const float2 wq = f2sub(mueq, mud);
+    const double wl = (double)wq.x + (live1 ? (double)wq.y : 0.0);
+    if ((int)((m0 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET) dspeed[g.aux[n0]] += (double)gin0 * s_t;
+    if (live1 && (int)((m1 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET)
+        dspeed[g.aux[n0 + 1]] += (double)gin1 * s_t;
+    return wl;
 }
 
 // Gadd (optional): the objective's term of this step per target, [target][Q],
@@ -852,15 +990,24 @@ __device__ __forceinline__ void pull_pair_body(const AGeom<float, Q>& g, const f
     const int n0 = bid * BLOCK_NODES + 2 * threadIdx.x;
     const unsigned ld = (unsigned)g.ld, u0 = (unsigned)n0;
     const bool live0 = n0 < g.n;
-    // the node's own f^t and word do not depend on the neighbour rows: load
-    // them first, so that their latency overlaps the staging of the block's
-    // segment rows in shared memory (one barrier, as the engine's kernels do)
+    // the node's own f^t and word do not depend on the neighbour rows: the
+    // moments of f^t are taken first, so that their loads overlap the staging
+    // of the block's segment rows in shared memory (one barrier, as the
+    // engine's kernels do), and f^t is not held in registers through the
+    // gather of lambda^{t+1}
     const MT m0 = live0 ? g.meta[n0] : MT(0);
     const MT m1 = n0 + 1 < g.n ? g.meta[n0 + 1] : MT(0);
-    float2 dpre[Q];
+    float2 ra = f2s(0.f), rb = f2s(0.f), j0 = f2s(0.f), j1 = f2s(0.f), j2 = f2s(0.f);
     if (live0) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) dpre[q] = *reinterpret_cast<const float2*>(D + (q * ld + u0));
+        for (int q = 0; q < Q; ++q) {
+            const float2 dq = *reinterpret_cast<const float2*>(D + (q * ld + u0));
+            if (q & 1) rb = f2add(rb, dq);
+            else ra = f2add(ra, dq);
+            if (L::cx(q)) j0 = L::cx(q) > 0 ? f2add(j0, dq) : f2sub(j0, dq);
+            if (L::cy(q)) j1 = L::cy(q) > 0 ? f2add(j1, dq) : f2sub(j1, dq);
+            if (L::cz(q)) j2 = L::cz(q) > 0 ? f2add(j2, dq) : f2sub(j2, dq);
+        }
     }
     {
         const int s0 = __ldg(g.seg_base + bid);
@@ -903,109 +1050,13 @@ __device__ __forceinline__ void pull_pair_body(const AGeom<float, Q>& g, const f
                 for (int q = 0; q < Q; ++q) mu[q].y = 0.f;
             }
         }
-        // moments of f^t and sum mu d, streaming the node's own slots
-        float2 ra = f2s(0.f), rb = f2s(0.f), j0 = f2s(0.f), j1 = f2s(0.f), j2 = f2s(0.f), mud = f2s(0.f);
+        // sum mu d: f^t read again, from L1 (the load is volatile so that the
+        // first read's values are not kept in registers instead)
+        float2 mud = f2s(0.f);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const float2 dq = dpre[q];
-            if (q & 1) rb = f2add(rb, dq);
-            else ra = f2add(ra, dq);
-            if (L::cx(q)) j0 = L::cx(q) > 0 ? f2add(j0, dq) : f2sub(j0, dq);
-            if (L::cy(q)) j1 = L::cy(q) > 0 ? f2add(j1, dq) : f2sub(j1, dq);
-            if (L::cz(q)) j2 = L::cz(q) > 0 ? f2add(j2, dq) : f2sub(j2, dq);
-            mud = f2fma(mu[q], dq, mud);
-        }
-        const float2 drho = f2add(ra, rb);
-        const float2 rho = f2add(f2s(1.f), drho);
-        const float2 irho = make_float2(1.f / rho.x, 1.f / rho.y);
-        const float2 u[3] = {f2mul(j0, irho), f2mul(j1, irho), f2mul(j2, irho)};
-        const float2 usq = f2fma(u[0], u[0], f2fma(u[1], u[1], f2mul(u[2], u[2])));
-        // outlet links: d/du of 2 w rho_out eq(u), times lambda = -mu (scalar, rare)
-        float2 G[3] = {f2s(0.f), f2s(0.f), f2s(0.f)};
-        if (ol0 | ol1) {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const float c0 = (float)L::cx(q), c1 = (float)L::cy(q), c2 = (float)L::cz(q);
-                const float k2 = (float)(2.0 * L::w(q) * g.out_rho);
-                if ((ol0 >> q) & 1) {
-                    const float cu = c0 * u[0].x + c1 * u[1].x + c2 * u[2].x;
-                    const float k = -mu[q].x * k2;
-                    G[0].x += k * (9.f * cu * c0 - 3.f * u[0].x);
-                    G[1].x += k * (9.f * cu * c1 - 3.f * u[1].x);
-                    G[2].x += k * (9.f * cu * c2 - 3.f * u[2].x);
-                }
-                if ((ol1 >> q) & 1) {
-                    const float cu = c0 * u[0].y + c1 * u[1].y + c2 * u[2].y;
-                    const float k = -mu[q].y * k2;
-                    G[0].y += k * (9.f * cu * c0 - 3.f * u[0].y);
-                    G[1].y += k * (9.f * cu * c1 - 3.f * u[1].y);
-                    G[2].y += k * (9.f * cu * c2 - 3.f * u[2].y);
-                }
-            }
-        }
-        // A = sum mu w (1 - 4.5 cu^2 + 1.5 u^2), B = sum mu w (3 + 9 cu) c - 3 u sum mu w,
-        // sum mu deq, over direction pairs (q, opp q): cu flips sign
-        const float2 base = f2fma(rho, f2mul(f2s(-1.5f), usq), drho);
-        const float2 rho3 = f2mul(f2s(3.f), rho);
-        const float2 a0 = f2fma(f2s(1.5f), usq, f2s(1.f));
-        float2 A = f2s(0.f), Wm = f2s(0.f), mueq = f2s(0.f);
-        float2 Bc[3] = {f2s(0.f), f2s(0.f), f2s(0.f)};
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int o = L::opp(q);
-            const float2 w = f2s((float)L::w(q));
-            if (q == L::REST) {
-                const float2 wm = f2mul(w, mu[q]);
-                A = f2fma(wm, a0, A);
-                Wm = f2add(Wm, wm);
-                mueq = f2fma(wm, base, mueq);
-                continue;
-            }
-            if (o < q) continue;
-            const float2 cu = cdot2<Q>(q, u);
-            const float2 mp = f2mul(w, f2add(mu[q], mu[o]));
-            const float2 mm = f2mul(w, f2sub(mu[q], mu[o]));
-            const float2 cu2 = f2mul(cu, cu);
-            A = f2fma(mp, f2fma(f2s(-4.5f), cu2, a0), A);
-            Wm = f2add(Wm, mp);
-            const float2 sym = f2fma(rho, f2mul(f2s(4.5f), cu2), base);
-            const float2 anti = f2mul(rho3, cu);
-            mueq = f2fma(sym, mp, f2fma(anti, mm, mueq));
-            // (3 mm + 9 cu mp) c
-            const float2 bk = f2fma(f2s(9.f), f2mul(cu, mp), f2mul(f2s(3.f), mm));
-            if (L::cx(q)) Bc[0] = L::cx(q) > 0 ? f2add(Bc[0], bk) : f2sub(Bc[0], bk);
-            if (L::cy(q)) Bc[1] = L::cy(q) > 0 ? f2add(Bc[1], bk) : f2sub(Bc[1], bk);
-            if (L::cz(q)) Bc[2] = L::cz(q) > 0 ? f2add(Bc[2], bk) : f2sub(Bc[2], bk);
-        }
-        const float2 B[3] = {f2fma(f2s(-3.f), f2mul(u[0], Wm), Bc[0]), f2fma(f2s(-3.f), f2mul(u[1], Wm), Bc[1]),
-                             f2fma(f2s(-3.f), f2mul(u[2], Wm), Bc[2])};
-        const float2 gu = f2fma(G[0], u[0], f2fma(G[1], u[1], f2mul(G[2], u[2])));
-        const float2 keep = f2s(1.f - g.omega), om = f2s(g.omega);
-        // lambda_q = (1 - omega) mu_q + omega (A + B.c_q) + (G.c_q - G.u) / rho
-        const float2 Ao = f2mul(om, A);
-        const float2 ngu = f2mul(f2s(-1.f), f2mul(gu, irho));
-        // targets among the two nodes (near-wall nodes are plain fluid nodes,
-        // aux = their near-wall entry)
-        int tk0 = -1, tk1 = -1;
-        if (Gadd) {
-            if ((m0 >> Meta<Q>::NW_SHIFT) & 1) tk0 = g.nw_target[g.aux[n0]];
-            if (live1 && ((m1 >> Meta<Q>::NW_SHIFT) & 1)) tk1 = g.nw_target[g.aux[n0 + 1]];
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const float2 bc = cdot2<Q>(q, B);
-            const float2 gc = cdot2<Q>(q, G);
-            float2 lam = f2fma(keep, mu[q], f2fma(om, bc, Ao));
-            lam = f2add(lam, f2fma(gc, irho, ngu));
-            if (tk0 >= 0) lam.x += Gadd[(long long)tk0 * Q + q];
-            if (tk1 >= 0) lam.y += Gadd[(long long)tk1 * Q + q];
-            *reinterpret_cast<float2*>(Lc + (q * ld + u0)) = lam;
-        }
-        const float2 wq = f2sub(mueq, mud);
-        wl = (double)wq.x + (live1 ? (double)wq.y : 0.0);
-        if ((int)((m0 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET) dspeed[g.aux[n0]] += (double)gin0 * s_t;
-        if (live1 && (int)((m1 >> Meta<Q>::KIND_SHIFT) & 3) == KIND_INLET)
-            dspeed[g.aux[n0 + 1]] += (double)gin1 * s_t;
+        for (int q = 0; q < Q; ++q) mud = f2fma(mu[q], reload2(D + (q * ld + u0)), mud);
+        wl = pull_pair_math<Q>(g, Lc, s_t, dspeed, Gadd, n0, live1, m0, m1, mu, ra, rb, j0, j1, j2, mud, gin0, gin1,
+                               ol0, ol1);
     }
     warp_accumulate(wl, domega);
 }

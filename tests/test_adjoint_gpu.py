@@ -257,3 +257,4 @@ def test_objective_staging_forms_agree(objective, monkeypatch):
     assert sg["J"] == st["J"]
     assert rel(sg["grad_coeffs"], st["grad_coeffs"]) < 1e-6
     assert abs(sg["dJ_dtau"] - st["dJ_dtau"]) <= 1e-6 * abs(st["dJ_dtau"])
+

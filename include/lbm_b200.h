@@ -450,6 +450,37 @@ typedef struct {
 /* Errors: lbm_last_error(NULL). */
 int lbm_config_parse(const char* path, lbm_config* out);
 
+/* ----------------------------------------------------- slab halo exchange ---
+ * Replaces the reference's six-face halo exchange of Simulation::Communicate
+ * (Simulation.cpp:270-516) over the Cartesian split of SubDomain
+ * (Subdomain.cpp:96-245) for a domain cut into slabs, one engine per slab
+ * (physics mode). A slab's engine holds its own nodes and, as plain fluid
+ * nodes in no list, the ghost copies of the other slabs' nodes next to them.
+ * Only the populations that cross a cut move: for the link set L of a pair of
+ * slabs A, B (node b of A, direction p, with b - c_p a node of B), the store
+ * that precedes a phase-1 step (the initialisation's or a phase-0 step's)
+ * leaves in slot p of b the value B's node pulls, and a phase-1 step leaves in
+ * B's ghost copy of b, slot p, the value b must receive. So after every step
+ * (and once before the first), by lbm_get_phase:
+ *   next_phase 1: A packs its list of (b, p) over its own nodes and sends it;
+ *                 B unpacks it into the same (b, p) of its ghosts;
+ *   next_phase 0: B packs that list over its ghosts and sends it back; A
+ *                 unpacks it into its own nodes.
+ * Both sides must define the list with the same entries in the same order.
+ *
+ * lbm_halo_define: list `id` (0..63) of n entries, node (caller index of this
+ * engine) and dir (0..Q-1); a list may be defined once. */
+int lbm_halo_define(lbm_engine* e, int32_t id, int64_t n, const int64_t* node, const int32_t* dir);
+
+/* Copies list `id`'s slots into dst / from src (device memory, n elements
+ * of the storage type: 8, 4 or 2 bytes), on the engine's stream. */
+int lbm_halo_pack(lbm_engine* e, int32_t id, void* dst);
+int lbm_halo_unpack(lbm_engine* e, int32_t id, const void* src);
+
+/* The phase of the next step: 1 after the initialisation and after a phase-0
+ * step, 0 after a phase-1 step. */
+int lbm_get_phase(lbm_engine* e, int32_t* next_phase);
+
 /* Message of the last failed call on e (or of the last failed lbm_create when
  * e is NULL). Never NULL. */
 const char* lbm_last_error(const lbm_engine* e);

@@ -362,6 +362,12 @@ struct lbm_engine {
     cudaEvent_t flag_ev = nullptr;     // recorded after the mirror's copy
     bool flag_copy_pending = false;
     bool numeric_fault = false;        // a completed copy showed FLAG_NONFINITE
+    // slab halo lists (lbm_halo_define): slot indices q * ld + internal node
+    struct HaloList {
+        int64_t n = -1;  // -1: not defined
+        long long* slots = nullptr;
+    };
+    HaloList halo[64];
 
     template <class T>
     cudaError_t alloc(T** p, size_t count) {
@@ -1305,6 +1311,97 @@ int lbm_get_info(lbm_engine* e, int64_t* n_nodes, int64_t* ld, int64_t* n_segmen
     if (n_nearwall) *n_nearwall = e->nw();
     if (n_outlet_nodes) *n_outlet_nodes = e->nout();
     if (device_bytes) *device_bytes = (int64_t)e->bytes;
+    return 0;
+}
+
+// ------------------------------------------------------ slab halo lists ---
+}  // extern "C"
+
+namespace {
+
+template <class T>
+__global__ void halo_pack_kernel(const T* __restrict__ pop, const long long* __restrict__ slots, long long n,
+                                 T* __restrict__ dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = pop[slots[i]];
+}
+
+template <class T>
+__global__ void halo_unpack_kernel(T* __restrict__ pop, const long long* __restrict__ slots, long long n,
+                                   const T* __restrict__ src) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pop[slots[i]] = src[i];
+}
+
+size_t storage_bytes(int storage) {
+    return storage == LBM_STORE_F64 ? 8 : storage == LBM_STORE_F32 ? 4 : 2;
+}
+
+int halo_copy(lbm_engine* e, int32_t id, void* buf, bool pack) {
+    if (!e || !buf || id < 0 || id >= 64) return LBM_ERR_ARGUMENT;
+    const auto& h = e->halo[id];
+    if (h.n < 0) return e->fail(LBM_ERR_STATE, "halo list " + std::to_string(id) + " is not defined");
+    if (h.n == 0) return 0;
+    cudaSetDevice(e->device);
+    const unsigned grid = (unsigned)((h.n + 255) / 256);
+    switch (storage_bytes(e->storage)) {
+        case 8:
+            if (pack) halo_pack_kernel<<<grid, 256, 0, e->stream>>>((const unsigned long long*)e->pop, h.slots, h.n,
+                                                                   (unsigned long long*)buf);
+            else halo_unpack_kernel<<<grid, 256, 0, e->stream>>>((unsigned long long*)e->pop, h.slots, h.n,
+                                                                (const unsigned long long*)buf);
+            break;
+        case 4:
+            if (pack) halo_pack_kernel<<<grid, 256, 0, e->stream>>>((const unsigned*)e->pop, h.slots, h.n,
+                                                                   (unsigned*)buf);
+            else halo_unpack_kernel<<<grid, 256, 0, e->stream>>>((unsigned*)e->pop, h.slots, h.n,
+                                                                (const unsigned*)buf);
+            break;
+        default:
+            if (pack) halo_pack_kernel<<<grid, 256, 0, e->stream>>>((const unsigned short*)e->pop, h.slots, h.n,
+                                                                   (unsigned short*)buf);
+            else halo_unpack_kernel<<<grid, 256, 0, e->stream>>>((unsigned short*)e->pop, h.slots, h.n,
+                                                                (const unsigned short*)buf);
+            break;
+    }
+    const cudaError_t ce = cudaGetLastError();
+    return ce == cudaSuccess ? 0 : e->cuda_fail(ce, pack ? "halo pack" : "halo unpack");
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_halo_define(lbm_engine* e, int32_t id, int64_t n, const int64_t* node, const int32_t* dir) {
+    if (!e) return LBM_ERR_ARGUMENT;
+    if (id < 0 || id >= 64) return e->fail(LBM_ERR_ARGUMENT, "halo list id out of range (0..63)");
+    if (e->halo[id].n >= 0) return e->fail(LBM_ERR_STATE, "halo list " + std::to_string(id) + " is already defined");
+    if (n < 0 || (n > 0 && (!node || !dir))) return e->fail(LBM_ERR_ARGUMENT, "bad halo list");
+    if (e->bc != LBM_BC_PHYSICS) return e->fail(LBM_ERR_STATE, "slab halo exchange needs physics boundaries");
+    std::vector<long long> slots((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        if (node[i] < 0 || node[i] >= e->t.n) return e->fail(LBM_ERR_ARGUMENT, "halo node index out of range");
+        if (dir[i] < 0 || dir[i] >= e->Q) return e->fail(LBM_ERR_ARGUMENT, "halo direction out of range");
+        slots[(size_t)i] = (long long)dir[i] * e->t.ld + e->t.iperm[(size_t)node[i]];
+    }
+    cudaSetDevice(e->device);
+    long long* d = nullptr;
+    const cudaError_t ce = e->upload(&d, slots);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "halo list");
+    e->halo[id].n = n;
+    e->halo[id].slots = d;
+    return 0;
+}
+
+int lbm_halo_pack(lbm_engine* e, int32_t id, void* dst) { return halo_copy(e, id, dst, true); }
+
+int lbm_halo_unpack(lbm_engine* e, int32_t id, const void* src) {
+    return halo_copy(e, id, const_cast<void*>(src), false);
+}
+
+int lbm_get_phase(lbm_engine* e, int32_t* next_phase) {
+    if (!e || !next_phase) return LBM_ERR_ARGUMENT;
+    *next_phase = e->phase;
     return 0;
 }
 

@@ -162,6 +162,10 @@ SIGNATURES = {
     "lbm_set_pulsatile": (ctypes.c_int, [_E, ctypes.POINTER(LbmPulseDesc)]),
     "lbm_pulse_eval": (ctypes.c_int, [ctypes.POINTER(LbmPulseDesc), ctypes.c_double, _f64p]),
     "lbm_config_parse": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(LbmConfig)]),
+    "lbm_halo_define": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_int64, _i64p, _i32p]),
+    "lbm_halo_pack": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_void_p]),
+    "lbm_halo_unpack": (ctypes.c_int, [_E, ctypes.c_int32, ctypes.c_void_p]),
+    "lbm_get_phase": (ctypes.c_int, [_E, _i32p]),
     "lbm_last_error": (ctypes.c_char_p, [_E]),
 }
 

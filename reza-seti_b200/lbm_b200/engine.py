@@ -149,6 +149,28 @@ class Engine:
         self._check(capi.lib().lbm_step_timed(self._h, int(n), ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    # ---- slab halo lists (lbm_halo_*)
+    def halo_define(self, list_id, nodes, dirs):
+        n = np.ascontiguousarray(nodes, dtype=np.int64)
+        d = np.ascontiguousarray(dirs, dtype=np.int32)
+        if len(n) != len(d):
+            raise ValueError("nodes and dirs differ in length")
+        self._keep["halo_%d" % list_id] = (n, d)
+        self._check(capi.lib().lbm_halo_define(self._h, int(list_id), len(n), _p(n, capi._i64p),
+                                                _p(d, capi._i32p)))
+
+    def halo_pack(self, list_id, dst_ptr):
+        """Copies list list_id's slots to device memory at dst_ptr (storage type)."""
+        self._check(capi.lib().lbm_halo_pack(self._h, int(list_id), ctypes.c_void_p(dst_ptr)))
+
+    def halo_unpack(self, list_id, src_ptr):
+        self._check(capi.lib().lbm_halo_unpack(self._h, int(list_id), ctypes.c_void_p(src_ptr)))
+
+    def next_phase(self):
+        v = ctypes.c_int32()
+        self._check(capi.lib().lbm_get_phase(self._h, ctypes.byref(v)))
+        return v.value
+
     # ---- results
     def time(self):
         s, r = ctypes.c_int64(), ctypes.c_double()

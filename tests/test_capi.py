@@ -47,6 +47,10 @@ def test_null_handle_calls_fail_cleanly():
     L = capi.lib()
     assert L.lbm_step(None, 1) == capi.LBM_ERR_ARGUMENT
     assert L.lbm_destroy(None) == capi.LBM_ERR_ARGUMENT
+    assert L.lbm_halo_define(None, 0, 0, None, None) == capi.LBM_ERR_ARGUMENT
+    assert L.lbm_halo_pack(None, 0, None) == capi.LBM_ERR_ARGUMENT
+    assert L.lbm_halo_unpack(None, 0, None) == capi.LBM_ERR_ARGUMENT
+    assert L.lbm_get_phase(None, None) == capi.LBM_ERR_ARGUMENT
     assert L.lbm_last_error(None)
 
 

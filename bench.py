@@ -120,10 +120,10 @@ def measured_peaks():
 # over the two phase kernels of one step, from an ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum on the step kernels (command
 # and case in profiles/step_kernel_traffic_d3q19.md); None where not captured.
-STEP_KERNEL_TRAFFIC = {"f32": 157.6, "f16": 82.07}
+STEP_KERNEL_TRAFFIC = {"f32": 156.2, "f16": 80.92}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one phase-0 and one phase-1 launch "
                   "on the default workload (21,381,419 nodes, 1.6 GB FP32 state, 13x L2), averaged: FP32 "
-                  "3.35 and 3.39 GB, FP16 1.741 and 1.769 GB per launch; the excess over the algorithmic "
+                  "3.33 and 3.35 GB, FP16 1.712 and 1.748 GB per launch; the excess over the algorithmic "
                   "2 Q S per node is the node words (4 B), segment rows and the near-wall hand-off")
 
 

@@ -19,7 +19,13 @@
  * The per-phase members keep their names and call order. The engine fuses a
  * whole step, so Collision() ... ApplyWallBc() only check the order and
  * ComputeWallShearStress(iter), the last phase of a reference step, runs the
- * step with the current InletVelocity_ and refreshes the Node fields.
+ * step with the current InletVelocity_ and refreshes the Node fields. The
+ * fields a reference phase would have changed by then hold NaN from that
+ * phase on, so that a caller reading them mid-step sees that they are not
+ * there instead of the previous step's values: Collision() sets density,
+ * velocity, velMag, m_eqdistributions and m_newDistributions; Streaming()
+ * m_distributions. ComputeWallShearStress restores all but
+ * m_newDistributions (the engine keeps no post-collision copy).
  *
  * LBM_B200_DUMP=<path>: after Iterate(), write the final Node fields in the
  * record format of the reference harness (oracle/refharness/harness.cpp), for
@@ -299,9 +305,33 @@ static void expect_phase(const Simulation* s, int want, int next, const char* na
     st.phase = next;
 }
 
-void Simulation::Collision() { expect_phase(this, 0, 1, "Collision"); }
+// Fields that the reference's phases change before the step's end: NaN
+// until ComputeWallShearStress has run the fused step.
+static void invalidate(const Simulation* s, bool collision) {
+    const double nan = std::nan("");
+    for (const auto& p : registry().at(s).nodes) {
+        Node& nd = *p;
+        if (collision) {
+            nd.density = nan;
+            for (int c = 0; c < 3; ++c) nd.velocity[c] = nan;
+            nd.velMag = nan;
+            for (auto& v : nd.m_eqdistributions) v = nan;
+            for (auto& v : nd.m_newDistributions) v = nan;
+        } else {
+            for (auto& v : nd.m_distributions) v = nan;
+        }
+    }
+}
+
+void Simulation::Collision() {
+    expect_phase(this, 0, 1, "Collision");
+    invalidate(this, true);
+}
 void Simulation::Communicate() {}
-void Simulation::Streaming() { expect_phase(this, 1, 2, "Streaming"); }
+void Simulation::Streaming() {
+    expect_phase(this, 1, 2, "Streaming");
+    invalidate(this, false);
+}
 void Simulation::ApplyZouHeBc() { expect_phase(this, 2, 3, "ApplyZouHeBc"); }
 void Simulation::ApplyInBc() {
     std::cerr << "B200 engine: ApplyInBc (never called by the reference loop) is not provided" << std::endl;

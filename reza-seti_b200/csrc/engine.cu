@@ -337,6 +337,7 @@ struct lbm_engine {
     double* obs_pop = nullptr;
     double* obs_mom[2] = {nullptr, nullptr};
     unsigned* flags = nullptr;
+    int* tile_sched = nullptr;  // [2] phase-1 tile counter, CTAs done (zero between launches)
     double* in_vel = nullptr;
     int* in_node = nullptr;    // internal index per inlet-list entry
     int* out_node = nullptr;   // internal index per outlet-table entry
@@ -436,6 +437,7 @@ StepArgs<S, Q> step_args(lbm_engine* e, double vel, double* mom) {
     a.obs_mom = mom;
     a.flags = e->flags;
     a.force_general = e->force_general ? 1 : 0;
+    a.tile_sched = e->tile_sched;
     return a;
 }
 
@@ -922,6 +924,7 @@ int create(const lbm_desc* d, lbm_engine** out) {
     for (auto& m : e->obs_mom)
         if ((ce = e->alloc(&m, (size_t)4 * t.ld)) != cudaSuccess) return bail(ce, "observation buffer");
     if ((ce = e->alloc(&e->flags, 1)) != cudaSuccess) return bail(ce, "flags");
+    if ((ce = e->alloc(&e->tile_sched, 2)) != cudaSuccess) return bail(ce, "tile counter");
     std::vector<double> zero_in((size_t)3 * std::max(1, e->nin()), 0.0);
     if ((ce = e->upload(&e->in_vel, zero_in)) != cudaSuccess) return bail(ce, "inlet profile");
     if ((ce = e->upload(&e->in_node, t.in_node)) != cudaSuccess) return bail(ce, "inlet list");
@@ -942,6 +945,7 @@ int create(const lbm_desc* d, lbm_engine** out) {
     cudaMemsetAsync(e->acc, 0, sizeof(double) * 3 * std::max(1, e->nw()), e->stream);
     cudaMemsetAsync(e->accmag, 0, sizeof(double) * std::max(1, e->nw()), e->stream);
     cudaMemsetAsync(e->flags, 0, sizeof(unsigned), e->stream);
+    cudaMemsetAsync(e->tile_sched, 0, 2 * sizeof(int), e->stream);
     // pad slots of the population buffer stay zero
     cudaMemsetAsync(e->pop, 0, (size_t)e->Q * t.ld * elem, e->stream);
     if ((ce = launch_fill_weights(e->obs_pop, t.ld, t.n, e->Q, e->stream)) != cudaSuccess)

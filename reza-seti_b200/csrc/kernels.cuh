@@ -116,6 +116,9 @@ struct StepArgs {
     // phase-1 pair kernel: 1 = every warp takes the per-node path, never the
     // twin path (LBM_B200_PHASE1_GENERAL=1; the two give identical results)
     int force_general;
+    // persistent phase-1 kernel: [0] the tile counter CTAs take their next
+    // tile from, [1] CTAs finished; the last CTA out zeroes both
+    int* tile_sched;
 };
 
 template <class S, int Q>
@@ -175,6 +178,17 @@ __device__ __forceinline__ void gather(const S* __restrict__ pop, long long ld, 
         s[q] = Store<S>::get(pop + idx);
     }
 }
+
+// ------------------------------------------ programmatic dependent launch ---
+// Physics-mode step and post kernels go out with programmatic stream
+// serialisation: a kernel's CTAs may be scheduled while the previous kernel
+// on the stream finishes. Each waits here (griddepcontrol.wait: until the
+// previous grid has completed and its writes are visible) before it reads
+// anything that kernel or an earlier one wrote; a kernel launched without
+// such a predecessor passes straight through. allow_next_grid lets the next
+// kernel's CTAs be scheduled once every CTA of this one has called it.
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // --------------------------------------------------------------- moments ---
 // FP64, reference operand order (Simulation.cpp:85-139 for D3Q19).
@@ -837,6 +851,8 @@ __global__ void boundary_kernel(BoundaryArgs<S, Q> a) {
 // trail the launch.
 template <class S, int Q>
 __global__ void post_kernel(BoundaryArgs<S, Q> b, OpenArgs<S, Q> o) {
+    allow_next_grid();
+    wait_prior_grid();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long n_open = (long long)o.n_in + o.n_out;
     if (i < n_open) {

@@ -7,6 +7,24 @@
 
 namespace lbm {
 
+// A launch with programmatic stream serialisation (the kernel must call
+// wait_prior_grid before it reads earlier kernels' results).
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <class S, int Q, int PHASE, int BC>
 static cudaError_t step_obs(const StepArgs<S, Q>& a, int obs, dim3 g, cudaStream_t st) {
     const int smem = PHASE == 1 ? a.seg_smem_bytes : 0;
@@ -21,13 +39,13 @@ static cudaError_t step_obs(const StepArgs<S, Q>& a, int obs, dim3 g, cudaStream
 
 template <class S, int Q>
 static cudaError_t pair_phase0(const StepArgs<S, Q>& a, int obs, dim3 g, cudaStream_t st) {
+    const dim3 b(PAIR_THREADS);
     switch (obs) {
-        case 0: pair_phase0_kernel<S, Q, 0><<<g, PAIR_THREADS, 0, st>>>(a); break;
-        case 1: pair_phase0_kernel<S, Q, 1><<<g, PAIR_THREADS, 0, st>>>(a); break;
-        case 2: pair_phase0_kernel<S, Q, 2><<<g, PAIR_THREADS, 0, st>>>(a); break;
-        default: pair_phase0_kernel<S, Q, 3><<<g, PAIR_THREADS, 0, st>>>(a); break;
+        case 0: return launch_pdl(pair_phase0_kernel<S, Q, 0>, g, b, 0, st, a);
+        case 1: return launch_pdl(pair_phase0_kernel<S, Q, 1>, g, b, 0, st, a);
+        case 2: return launch_pdl(pair_phase0_kernel<S, Q, 2>, g, b, 0, st, a);
+        default: return launch_pdl(pair_phase0_kernel<S, Q, 3>, g, b, 0, st, a);
     }
-    return cudaGetLastError();
 }
 
 // Persistent phase-1 pair kernel: one CTA per resident slot (SM count times
@@ -55,8 +73,7 @@ static cudaError_t pair_phase1_launch(const StepArgs<S, Q>& a, cudaStream_t st) 
         cached_smem = smem;
     }
     const int grid = n_tiles < cached_grid ? n_tiles : cached_grid;
-    kern<<<grid, PAIR_THREADS, smem, st>>>(a, n_tiles);
-    return cudaGetLastError();
+    return launch_pdl(kern, dim3(grid), dim3(PAIR_THREADS), smem, st, a, n_tiles);
 }
 
 template <class S, int Q>
@@ -121,8 +138,7 @@ cudaError_t launch_post(const BoundaryArgs<S, Q>& b, const OpenArgs<S, Q>& o, cu
     const long long items = (long long)b.n_wss + o.n_in + o.n_out;
     if (items == 0) return cudaSuccess;
     const int tpb = 128;
-    post_kernel<S, Q><<<(unsigned)((items + tpb - 1) / tpb), tpb, 0, st>>>(b, o);
-    return cudaGetLastError();
+    return launch_pdl(post_kernel<S, Q>, dim3((unsigned)((items + tpb - 1) / tpb)), dim3(tpb), 0, st, b, o);
 }
 
 #define LBM_INSTANTIATE(S, Q)                                                                          \

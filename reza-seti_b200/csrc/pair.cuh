@@ -320,11 +320,17 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair0_min_blocks<S, Q>()) pair_p
     using L = Lat<Q>;
     using MT = typename Meta<Q>::T;
     using IO = PairIO<S>;
+    allow_next_grid();
     const int n0 = blockIdx.x * BLOCK_NODES + 2 * threadIdx.x;
-    if (n0 >= a.n) return;
+    if (n0 >= a.n) {
+        wait_prior_grid();
+        return;
+    }
     const bool live1 = n0 + 1 < a.n;
+    // node words never change: read before the wait
     const MT m0 = a.meta[n0];
     const MT m1 = live1 ? a.meta[n0 + 1] : MT(0);
+    wait_prior_grid();
     float2 s[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) s[q] = IO::get2(a.pop + (q * (unsigned)a.ld + (unsigned)n0));
@@ -408,14 +414,25 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_p
         cp_async_commit();
     };
 
+    // a CTA's first tile is its index; the later ones come from a counter
+    // (one atomic per tile, taken a tile ahead), so that CTAs that finish
+    // early take more tiles instead of every CTA walking the same stride
+    __shared__ int sched[2];
+    allow_next_grid();
     int tile = blockIdx.x;
-    if (tile >= n_tiles) return;
-    int b = 0;
+    if (tile >= n_tiles) {
+        wait_prior_grid();
+        return;
+    }
+    int b = 0, sb = 1;
+    // node words and segment rows never change: copied before the wait
     prefetch(tile, 0);
+    wait_prior_grid();
+    if (tid == 0) sched[0] = gridDim.x + atomicAdd(a.tile_sched, 1);
     cp_async_wait_all();
     __syncthreads();
+    int next = sched[0];
     for (;;) {
-        const int next = tile + gridDim.x;
         const int n0 = tile * BLOCK_NODES + 2 * tid;
         const bool live0 = n0 < a.n, live1 = n0 + 1 < a.n;
         const MT m0 = meta_buf(b)[2 * tid];
@@ -430,7 +447,10 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_p
         float2 s[Q];
         if (uniform) pair_gather1_twin<S, Q>(a, s, m0, sd0, n0);
         else pair_gather1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
-        if (next < n_tiles) prefetch(next, b ^ 1);
+        if (next < n_tiles) {
+            prefetch(next, b ^ 1);
+            if (tid == 0) sched[sb] = gridDim.x + atomicAdd(a.tile_sched, 1);
+        }
         if (live0) {
             pair_middle<S, Q, OBS>(a, s, m0, m1, n0, live1);
             if (uniform) pair_scatter1_twin<S, Q>(a, s, m0, sd0, n0);
@@ -440,7 +460,19 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_p
         cp_async_wait_all();
         __syncthreads();
         tile = next;
+        next = sched[sb];
+        sb ^= 1;
         b ^= 1;
+    }
+    // the last CTA out leaves the counter at zero for the next launch (the
+    // launches of one engine are ordered on its stream); the fence orders
+    // this CTA's counter updates before its count of finished CTAs
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(a.tile_sched + 1, 1) == (int)gridDim.x - 1) {
+            a.tile_sched[0] = 0;
+            a.tile_sched[1] = 0;
+        }
     }
 }
 

@@ -222,7 +222,10 @@ int lbm_get_flags(lbm_engine* e, uint32_t* flags);
  * The events are recorded around a sample of the steps (the two that begin
  * every 32 steps, one of each phase), and the sums are the sampled averages
  * times n_steps: an event between every pair of kernels would add about 10 us
- * of device time to each step. */
+ * of device time to each step. In physics mode a step's kernels overlap the
+ * previous kernel's tail (programmatic dependent launch), except around the
+ * sampled steps, so the two sums can exceed the call's device time: time the
+ * call itself for throughput. */
 int lbm_step_timed(lbm_engine* e, int64_t n_steps, double* step_kernel_ms, double* boundary_kernel_ms);
 
 /* Sizes: nodes, padded leading dimension, segments, near-wall nodes, outlet

@@ -752,6 +752,8 @@ __device__ __forceinline__ void push_pair_body(const AGeom<float, Q>& g, const f
     const bool live0 = n0 < g.n, live1 = n0 + 1 < g.n;
     const MT m0 = live0 ? g.meta[n0] : MT(0);
     const MT m1 = live1 ? g.meta[n0 + 1] : MT(0);
+    // node words never change; the state comes from the previous launch
+    wait_prior_grid();
     // a warp whose every pair is a twin takes the twin path; mixed warps take
     // the general one, which serves twins too, instead of running both
     const bool twin = __all_sync(0xffffffffu, !live0 || adj_twin<Q>(m0, m1));
@@ -792,6 +794,7 @@ __device__ __forceinline__ void push_pair_body(const AGeom<float, Q>& g, const f
 template <int Q>
 __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
     adj_push_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t) {
+    allow_next_grid();
     push_pair_body<Q>(g, D, Dn, s_t, blockIdx.x);
 }
 
@@ -804,7 +807,9 @@ template <int Q, bool THREADS>
 __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
     adj_push_objective_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t,
                               ObjArgs<float, Q> a, int t, int obj_blocks) {
+    allow_next_grid();
     if ((int)blockIdx.x < obj_blocks) {
+        wait_prior_grid();
         if (THREADS) objective_thread_body<float, Q>(a, D, t, blockIdx.x);
         else objective_warp_body<float, Q>(a, D, t, blockIdx.x);
     } else {
@@ -997,6 +1002,8 @@ __device__ __forceinline__ void pull_pair_body(const AGeom<float, Q>& g, const f
     // gather of lambda^{t+1}
     const MT m0 = live0 ? g.meta[n0] : MT(0);
     const MT m1 = n0 + 1 < g.n ? g.meta[n0 + 1] : MT(0);
+    // node words never change; f^t and lambda^{t+1} come from earlier launches
+    wait_prior_grid();
     float2 ra = f2s(0.f), rb = f2s(0.f), j0 = f2s(0.f), j1 = f2s(0.f), j2 = f2s(0.f);
     if (live0) {
 #pragma unroll
@@ -1066,6 +1073,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PULL_MIN_BLOCKS)
     adj_pull_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
                          float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
                          double* __restrict__ domega, const float* __restrict__ Gadd) {
+    allow_next_grid();
     pull_pair_body<Q>(g, D, Ln, Lc, s_t, dspeed, domega, Gadd, blockIdx.x);
 }
 
@@ -1258,7 +1266,9 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     auto push_on = [&](cudaStream_t stream, const R* D, R* Dn, int64_t t) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
-                adj_push_pair_kernel<Q><<<pgrid, PAIR_THREADS, 0, stream>>>(g, D, Dn, s.factors[t]);
+                const cudaError_t e = launch_pdl(adj_push_pair_kernel<Q>, pgrid, dim3(PAIR_THREADS), 0, stream, g, D,
+                                                 Dn, s.factors[t]);
+                (void)e;  // launch errors surface through cudaGetLastError after the sweep
                 return;
             }
         }
@@ -1268,8 +1278,9 @@ int run(const AdjointSetup& s, AdjointOut& o) {
     auto pull = [&](const R* D, const R* Ln, R* Lc, int64_t t, const R* Gadd) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
-                adj_pull_pair_kernel<Q><<<pgrid, PAIR_THREADS, pull_smem, st>>>(g, D, Ln, Lc, s.factors[t], dspeed,
-                                                                                  scal + N_PARTIALS, Gadd);
+                const cudaError_t e = launch_pdl(adj_pull_pair_kernel<Q>, pgrid, dim3(PAIR_THREADS), (size_t)pull_smem, st,
+                                                 g, D, Ln, Lc, s.factors[t], dspeed, scal + N_PARTIALS, Gadd);
+                (void)e;  // launch errors surface through cudaGetLastError after the sweep
                 return;
             }
         }
@@ -1286,12 +1297,14 @@ int run(const AdjointSetup& s, AdjointOut& o) {
             if (pairs && nt) {
                 const int ob = (int)(obj_threads ? tgrid_t : tgrid);
                 const dim3 fgrid(pgrid.x + (unsigned)ob);
+                cudaError_t e;
                 if (obj_threads)
-                    adj_push_objective_kernel<Q, true><<<fgrid, PAIR_THREADS, 0, st>>>(g, D, Dn, s.factors[t], oa,
-                                                                                        (int)t, ob);
+                    e = launch_pdl(adj_push_objective_kernel<Q, true>, fgrid, dim3(PAIR_THREADS), 0, st, g, D, Dn,
+                                   s.factors[t], oa, (int)t, ob);
                 else
-                    adj_push_objective_kernel<Q, false><<<fgrid, PAIR_THREADS, 0, st>>>(g, D, Dn, s.factors[t], oa,
-                                                                                         (int)t, ob);
+                    e = launch_pdl(adj_push_objective_kernel<Q, false>, fgrid, dim3(PAIR_THREADS), 0, st, g, D, Dn,
+                                   s.factors[t], oa, (int)t, ob);
+                (void)e;  // launch errors surface through cudaGetLastError after the sweep
                 return;
             }
         }

@@ -7,24 +7,6 @@
 
 namespace lbm {
 
-// A launch with programmatic stream serialisation (the kernel must call
-// wait_prior_grid before it reads earlier kernels' results).
-template <class... KArgs, class... Args>
-static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                              Args... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, args...);
-}
-
 template <class S, int Q, int PHASE, int BC>
 static cudaError_t step_obs(const StepArgs<S, Q>& a, int obs, dim3 g, cudaStream_t st) {
     const int smem = PHASE == 1 ? a.seg_smem_bytes : 0;

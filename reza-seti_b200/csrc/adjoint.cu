@@ -1328,9 +1328,19 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         for (int64_t sg = 0; sg < nseg; ++sg) {
             const int64_t t0 = sg * K, t1 = std::min(T, t0 + K);
             seg[0] = ck[sg];
-            for (int64_t t = t0; t < t1; ++t) objective_push(seg[t - t0], seg[t - t0 + 1], t);
-            if (sg + 1 < nseg)
-                cudaMemcpyAsync(ck[sg + 1], seg[t1 - t0], field * sizeof(R), cudaMemcpyDeviceToDevice, st);
+            if (sg + 1 < nseg) {
+                // of this segment only the next checkpoint is kept: the steps
+                // alternate between two buffers (a state the size of L2 stays
+                // there) and the last one writes the checkpoint itself
+                const R* src = ck[sg];
+                for (int64_t t = t0; t < t1; ++t) {
+                    R* dst = t + 1 == t1 ? ck[sg + 1] : seg[1 + ((t - t0) & 1)];
+                    objective_push(src, dst, t);
+                    src = dst;
+                }
+            } else {
+                for (int64_t t = t0; t < t1; ++t) objective_push(seg[t - t0], seg[t - t0 + 1], t);
+            }
         }
         const int64_t tl = (nseg - 1) * K;
         objective(seg[T - tl], T);

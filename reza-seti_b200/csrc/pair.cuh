@@ -63,7 +63,8 @@ constexpr int PAIR_THREADS = BLOCK_NODES / 2;
 // Its loads carry no dependency, so occupancy is what keeps bytes in flight:
 // 6 CTAs (80 registers) for FP32, 8 (64 registers) for the 16-bit types,
 // whose 2-wide loads move half the bytes per instruction. D3Q27 holds 27
-// pairs of values and gets its own caps.
+// pairs of values and gets its own caps: 5 CTAs (96 registers, no spills)
+// for every storage type (FP32 at 4 was 2 % slower on the bifurcation).
 template <class S, int Q>
 constexpr int pair0_min_blocks() {
 #ifdef LBM_PAIR0_MIN_BLOCKS
@@ -73,7 +74,7 @@ constexpr int pair0_min_blocks() {
 #ifdef LBM_PAIR0_MIN_BLOCKS_Q27
         return LBM_PAIR0_MIN_BLOCKS_Q27;
 #else
-        return sizeof(S) == 4 ? 4 : 5;
+        return 5;
 #endif
     }
     return sizeof(S) == 4 ? 6 : 8;

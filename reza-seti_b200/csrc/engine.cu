@@ -322,6 +322,7 @@ struct lbm_engine {
     void* meta = nullptr;
     int* seg_base = nullptr;
     int* seg_delta = nullptr;
+    int* seg_slot = nullptr;   // shifted storage: [segments][Q] d * ld + delta (pair phase-1 kernel)
     int* aux = nullptr;
     int* out_src = nullptr;
     void* out_buf = nullptr;
@@ -423,6 +424,7 @@ StepArgs<S, Q> step_args(lbm_engine* e, double vel, double* mom) {
     a.meta = (const typename Meta<Q>::T*)e->meta;
     a.seg_base = e->seg_base;
     a.seg_delta = e->seg_delta;
+    a.seg_slot = e->seg_slot;
     a.seg_smem_bytes = e->t.max_block_segs * Q * (int)sizeof(int);
     a.aux = e->aux;
     a.omega = (C)e->omega;
@@ -893,6 +895,17 @@ int create(const lbm_desc* d, lbm_engine** out) {
     }
     if ((ce = e->upload(&e->seg_base, t.seg_base)) != cudaSuccess) return bail(ce, "segments");
     if ((ce = e->upload(&e->seg_delta, t.seg_delta)) != cudaSuccess) return bail(ce, "segments");
+    if (e->shifted()) {
+        // the pair phase-1 kernel's row entry for direction d is the slot
+        // offset d * ld + delta, taken modulo 2^32 (its slot indices are
+        // 32-bit; the launcher requires Q * ld < 2^32 for that kernel)
+        std::vector<int> slot(t.seg_delta.size());
+        for (size_t i = 0; i < slot.size(); ++i) {
+            const uint32_t d = (uint32_t)(i % (size_t)e->Q);
+            slot[i] = (int)(d * (uint32_t)t.ld + (uint32_t)t.seg_delta[i]);
+        }
+        if ((ce = e->upload(&e->seg_slot, slot)) != cudaSuccess) return bail(ce, "segments");
+    }
     if ((ce = e->upload(&e->aux, t.aux)) != cudaSuccess) return bail(ce, "aux");
     if ((ce = e->upload(&e->out_src, t.out_src)) != cudaSuccess) return bail(ce, "outlets");
     if ((ce = e->upload(&e->out_nrm, t.out_nrm)) != cudaSuccess) return bail(ce, "outlets");

@@ -90,6 +90,9 @@ struct StepArgs {
     const MT* meta;
     const int* seg_base;   // [blocks] first segment of each block
     const int* seg_delta;  // [segments][Q] neighbour index offsets
+    // shifted storage: [segments][Q] slot offsets d * ld + delta (mod 2^32),
+    // the rows of the pair phase-1 kernel (one add per slot index)
+    const int* seg_slot;
     int seg_smem_bytes;    // shared memory for the largest block's segment rows
     const int* aux;        // [n] index into the inlet / outlet / near-wall tables
     C omega;               // 1 / tau

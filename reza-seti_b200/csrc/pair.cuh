@@ -238,8 +238,8 @@ __device__ __forceinline__ void pair_gather1(const StepArgs<S, Q>& a, float2 s[Q
         } else {
             const int oq = L::opp(q);
             const unsigned own0 = q * ld + u0;
-            const unsigned i0 = ((m0 >> oq) & 1) ? oq * ld + (unsigned)(n0 + sd0[oq]) : own0;
-            const unsigned i1 = ((m1 >> oq) & 1) ? oq * ld + (unsigned)(n0 + 1 + sd1[oq]) : own0 + 1;
+            const unsigned i0 = ((m0 >> oq) & 1) ? u0 + (unsigned)sd0[oq] : own0;
+            const unsigned i1 = ((m1 >> oq) & 1) ? u0 + 1u + (unsigned)sd1[oq] : own0 + 1;
             s[q] = make_float2(IO::get(a.pop + i0), IO::get(a.pop + i1));
         }
     }
@@ -261,8 +261,8 @@ __device__ __forceinline__ void pair_scatter1(const StepArgs<S, Q>& a, const flo
         }
         const int oq = L::opp(q);
         const unsigned own0 = oq * ld + u0;
-        const unsigned i0 = ((m0 >> q) & 1) ? q * ld + (unsigned)(n0 + sd0[q]) : own0;
-        const unsigned i1 = ((m1 >> q) & 1) ? q * ld + (unsigned)(n0 + 1 + sd1[q]) : own0 + 1;
+        const unsigned i0 = ((m0 >> q) & 1) ? u0 + (unsigned)sd0[q] : own0;
+        const unsigned i1 = ((m1 >> q) & 1) ? u0 + 1u + (unsigned)sd1[q] : own0 + 1;
         IO::put(a.pop + i0, s[q].x);
         IO::put(a.pop + i1, s[q].y);
     }
@@ -282,7 +282,7 @@ __device__ __forceinline__ void pair_gather1_twin(const StepArgs<S, Q>& a, float
             s[q] = IO::get2(a.pop + (q * ld + u0));
         } else {
             const int oq = L::opp(q);
-            const unsigned i = ((m >> oq) & 1) ? oq * ld + (unsigned)(n0 + sd[oq]) : q * ld + u0;
+            const unsigned i = ((m >> oq) & 1) ? u0 + (unsigned)sd[oq] : q * ld + u0;
             const S* p = a.pop + i;
             // an even slot index is 2-wide aligned: one access for both nodes
             if (i & 1) s[q] = make_float2(IO::get(p), IO::get(p + 1));
@@ -304,7 +304,7 @@ __device__ __forceinline__ void pair_scatter1_twin(const StepArgs<S, Q>& a, cons
             continue;
         }
         const int oq = L::opp(q);
-        const unsigned i = ((m >> q) & 1) ? q * ld + (unsigned)(n0 + sd[q]) : oq * ld + u0;
+        const unsigned i = ((m >> q) & 1) ? u0 + (unsigned)sd[q] : oq * ld + u0;
         S* p = a.pop + i;
         if (i & 1) {
             IO::put(p, s[q].x);
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_p
         else cp_async_16(meta_buf(b) + 2 * tid, src);
         const int s0 = __ldg(a.seg_base + tile);
         const int cnt = (__ldg(a.seg_base + tile + 1) - s0) * Q;
-        const int* rows = a.seg_delta + (long long)s0 * Q;
+        const int* rows = a.seg_slot + (long long)s0 * Q;
         int* dst = rows_buf(b);
         for (int i = tid; i < cnt; i += PAIR_THREADS) cp_async_4(dst + i, rows + i);
         cp_async_commit();

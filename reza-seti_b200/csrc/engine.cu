@@ -322,7 +322,7 @@ struct lbm_engine {
     void* meta = nullptr;
     int* seg_base = nullptr;
     int* seg_delta = nullptr;
-    int* seg_slot = nullptr;   // shifted storage: [segments][Q] d * ld + delta (pair phase-1 kernel)
+    int* seg_slot = nullptr;   // pair phase-1 kernel: [segments][Q] d * ld + delta (mod 2^32)
     int* aux = nullptr;
     int* out_src = nullptr;
     void* out_buf = nullptr;
@@ -895,10 +895,10 @@ int create(const lbm_desc* d, lbm_engine** out) {
     }
     if ((ce = e->upload(&e->seg_base, t.seg_base)) != cudaSuccess) return bail(ce, "segments");
     if ((ce = e->upload(&e->seg_delta, t.seg_delta)) != cudaSuccess) return bail(ce, "segments");
-    if (e->shifted()) {
+    if (e->shifted() && e->bc == LBM_BC_PHYSICS && (long long)e->Q * t.ld < (1LL << 32)) {
         // the pair phase-1 kernel's row entry for direction d is the slot
         // offset d * ld + delta, taken modulo 2^32 (its slot indices are
-        // 32-bit; the launcher requires Q * ld < 2^32 for that kernel)
+        // 32-bit; the launcher runs it only when Q * ld < 2^32)
         std::vector<int> slot(t.seg_delta.size());
         for (size_t i = 0; i < slot.size(); ++i) {
             const uint32_t d = (uint32_t)(i % (size_t)e->Q);
@@ -1427,10 +1427,6 @@ const char* lbm_last_error(const lbm_engine* e) { return e ? e->err.c_str() : g_
 }  // extern "C"
 
 void lbm::set_global_error(const std::string& msg) { g_create_error = msg; }
-
-extern "C" {
-
-}  // extern "C"
 
 namespace lbm {
 // Caller-order node coordinates and near-wall list of an engine, for the

@@ -152,6 +152,22 @@ int lbm_set_observation(lbm_engine* e, int32_t enabled);
 /* Steps taken so far, and the flow clock (total_runtime). */
 int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime);
 
+/* Restart support. The reference writes no restart files, so these three have
+ * no counterpart in it. The state the next step reads is copied as one host
+ * blob of lbm_state_size bytes. It holds the stored populations (storage type,
+ * internal layout), the near-wall moments the next wall shear stress uses, the
+ * WSS with its FP64 accumulators, the step count, the flow clock and the AA
+ * phase. lbm_get_state copies it out; a whole step must have been taken
+ * (always the case between calls). lbm_set_state puts it into an engine built
+ * from the same node set with the same lattice, storage type and boundary
+ * mode; other blobs are refused with LBM_ERR_ARGUMENT. With the caller's flow
+ * settings set again, the steps then continue bit for bit. Populations,
+ * moments and fluxes are readable again after the next step (LBM_ERR_STATE
+ * before it); WSS and OSI/TAWSS at once. */
+int lbm_state_size(lbm_engine* e, int64_t* bytes);
+int lbm_get_state(lbm_engine* e, void* dst);
+int lbm_set_state(lbm_engine* e, const void* src);
+
 /* Node::m_distributions after the last step (post-boundary populations),
  * [n_nodes][q] in the caller's node order. */
 int lbm_get_populations(lbm_engine* e, double* f);

@@ -1108,6 +1108,121 @@ int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime) {
     return 0;
 }
 
+}  // extern "C"
+
+// Restart support: the state the next step reads, as one host blob.
+namespace {
+struct StateHeader {
+    uint32_t magic, version;
+    int32_t lattice, storage, bc, phase;
+    int64_t n, ld, n_nw, n_segments, step;
+    double runtime;
+    int64_t pop_bytes, mom_bytes;
+};
+constexpr uint32_t STATE_MAGIC = 0x534d424cu;  // "LBMS"
+constexpr uint32_t STATE_VERSION = 1;
+
+StateHeader state_header(const lbm_engine* e) {
+    StateHeader h{};
+    h.magic = STATE_MAGIC;
+    h.version = STATE_VERSION;
+    h.lattice = e->Q;
+    h.storage = e->storage;
+    h.bc = e->bc;
+    h.phase = e->phase;
+    h.n = e->t.n;
+    h.ld = e->t.ld;
+    h.n_nw = e->nw();
+    h.n_segments = e->t.nseg;
+    h.step = e->step;
+    h.runtime = e->runtime;
+    const int64_t elem = e->storage == LBM_STORE_F64 ? 8 : (e->storage == LBM_STORE_F32 ? 4 : 2);
+    h.pop_bytes = (int64_t)e->Q * e->t.ld * elem;
+    h.mom_bytes = 4 * h.n_nw * (e->storage == LBM_STORE_F64 ? 8 : 4);
+    return h;
+}
+
+int64_t state_bytes(const StateHeader& h) {
+    return (int64_t)sizeof(StateHeader) + h.pop_bytes + h.mom_bytes + 5 * 8 * h.n_nw;
+}
+}  // namespace
+
+extern "C" {
+
+int lbm_state_size(lbm_engine* e, int64_t* bytes) {
+    if (!e || !bytes) return LBM_ERR_ARGUMENT;
+    *bytes = state_bytes(state_header(e));
+    return 0;
+}
+
+int lbm_get_state(lbm_engine* e, void* dst) {
+    if (!e || !dst) return LBM_ERR_ARGUMENT;
+    if (e->wss_pending) return e->fail(LBM_ERR_STATE, "lbm_get_state: a wall shear stress reduction is pending");
+    cudaSetDevice(e->device);
+    const StateHeader h = state_header(e);
+    char* p = static_cast<char*>(dst);
+    std::memcpy(p, &h, sizeof h);
+    p += sizeof h;
+    const size_t m = (size_t)h.n_nw;
+    struct Part { const void* src; size_t bytes; } parts[] = {
+        {e->pop, (size_t)h.pop_bytes}, {e->nw_mom, (size_t)h.mom_bytes}, {e->wss, 8 * m},
+        {e->acc, 24 * m}, {e->accmag, 8 * m}};
+    for (const Part& part : parts) {
+        if (part.bytes) {
+            cudaError_t ce = cudaMemcpyAsync(p, part.src, part.bytes, cudaMemcpyDeviceToHost, e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "state download");
+        }
+        p += part.bytes;
+    }
+    return sync(e);
+}
+
+int lbm_set_state(lbm_engine* e, const void* src) {
+    if (!e || !src) return LBM_ERR_ARGUMENT;
+    StateHeader h;
+    std::memcpy(&h, src, sizeof h);
+    const StateHeader mine = state_header(e);
+    if (h.magic != STATE_MAGIC || h.version != STATE_VERSION)
+        return e->fail(LBM_ERR_ARGUMENT, "lbm_set_state: not a state blob of this version");
+    if (h.lattice != mine.lattice || h.storage != mine.storage || h.bc != mine.bc || h.n != mine.n ||
+        h.ld != mine.ld || h.n_nw != mine.n_nw || h.n_segments != mine.n_segments ||
+        h.pop_bytes != mine.pop_bytes || h.mom_bytes != mine.mom_bytes)
+        return e->fail(LBM_ERR_ARGUMENT,
+                       "lbm_set_state: the state comes from an engine with another node set, lattice, "
+                       "storage type or boundary mode");
+    if (h.phase != 0 && h.phase != 1) return e->fail(LBM_ERR_ARGUMENT, "lbm_set_state: bad phase");
+    cudaSetDevice(e->device);
+    if (int rc = sync(e)) return rc;
+    const char* p = static_cast<const char*>(src) + sizeof h;
+    const size_t m = (size_t)h.n_nw;
+    struct Part { void* dst; size_t bytes; } parts[] = {
+        {e->pop, (size_t)h.pop_bytes}, {e->nw_mom, (size_t)h.mom_bytes}, {e->wss, 8 * m},
+        {e->acc, 24 * m}, {e->accmag, 8 * m}};
+    for (const Part& part : parts) {
+        if (part.bytes) {
+            cudaError_t ce = cudaMemcpyAsync(part.dst, p, part.bytes, cudaMemcpyHostToDevice, e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "state upload");
+        }
+        p += part.bytes;
+    }
+    cudaError_t cm = cudaMemsetAsync(e->flags, 0, sizeof(unsigned), e->stream);
+    if (cm != cudaSuccess) return e->cuda_fail(cm, "flags");
+    if (int rc = sync(e)) return rc;
+    e->step = h.step;
+    e->runtime = h.runtime;
+    e->phase = h.phase;
+    e->flag_copy_pending = false;
+    e->numeric_fault = false;
+    e->wss_pending = false;
+    // the observation buffers hold nothing of the restored state: populations,
+    // moments and fluxes are available again after the next step
+    e->pop_step = -1;
+    e->mom_step[0] = e->mom_step[1] = -1;
+    // a restored state is not an initialisation: setters must not redo it
+    e->fresh = false;
+    return 0;
+}
+
 int lbm_get_populations(lbm_engine* e, double* f) {
     if (!e || !f) return LBM_ERR_ARGUMENT;
     if (e->pop_step != e->step) return e->fail(LBM_ERR_STATE, "populations of the last step were not observed");

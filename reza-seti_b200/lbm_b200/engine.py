@@ -42,6 +42,8 @@ class Engine:
                  bc="reference", device=0, numeric_check=True):
         L = capi.lib()
         self.q = lattice
+        self.storage = storage
+        self.bc = bc
         keep = {}
         keep["coords"] = np.ascontiguousarray(topo["coords"], dtype=np.int32).reshape(-1, 3)
         keep["kind"] = np.ascontiguousarray(topo["kind"], dtype=np.uint8)
@@ -177,6 +179,24 @@ class Engine:
         self._check(capi.lib().lbm_get_time(self._h, ctypes.byref(s), ctypes.byref(r)))
         return s.value, r.value
 
+    def get_state(self):
+        """The state the next step reads, as bytes (lbm_get_state)."""
+        size = ctypes.c_int64()
+        self._check(capi.lib().lbm_state_size(self._h, ctypes.byref(size)))
+        buf = np.empty(size.value, dtype=np.uint8)
+        self._check(capi.lib().lbm_get_state(self._h, buf.ctypes.data))
+        return buf
+
+    def set_state(self, blob):
+        """Restores a state from get_state of an engine like this one
+        (lbm_set_state); the steps then continue bit for bit."""
+        size = ctypes.c_int64()
+        self._check(capi.lib().lbm_state_size(self._h, ctypes.byref(size)))
+        buf = np.ascontiguousarray(blob, dtype=np.uint8).reshape(-1)
+        if buf.size != size.value:
+            raise ValueError("state of %d bytes, this engine's is %d" % (buf.size, size.value))
+        self._check(capi.lib().lbm_set_state(self._h, buf.ctypes.data))
+
     def populations(self, out=None):
         f = np.empty((self.n, self.q)) if out is None else out
         self._check(capi.lib().lbm_get_populations(self._h, f.ctypes.data))
@@ -196,6 +216,18 @@ class Engine:
         w, a, am = np.empty(m), np.empty((m, 3)), np.empty(m)
         self._check(capi.lib().lbm_get_wss(self._h, w.ctypes.data, a.ctypes.data, am.ctypes.data))
         return w, a, am
+
+    def save_checkpoint(self, path):
+        """Writes the state a resumed run needs to path (lbm_b200.checkpoint)."""
+        from . import checkpoint
+        checkpoint.save(self, path)
+
+    def load_checkpoint(self, path):
+        """Restores a checkpoint written by save_checkpoint from an engine of
+        the same topology, lattice, storage type and boundary mode, after the
+        flow settings; the run then continues as if it had not stopped."""
+        from . import checkpoint
+        checkpoint.restore(self, checkpoint.read(path))
 
     def osi_tawss(self):
         m = self.n_nearwall

@@ -1,0 +1,136 @@
+"""Checkpoint files on the CPU: the format round-trips, and every kind of
+damage is refused with CheckpointError before anything reaches an engine.
+The damage covered: a flipped bit (CRC-32), truncation, a foreign file, another
+format version, trailing bytes, a missing array. Also checked: a checkpoint is
+refused by an engine unlike its writer, and restore() hands the engine the
+state blob. A stand-in records the calls; no GPU is used."""
+import json
+import struct
+import types
+
+import numpy as np
+import pytest
+
+from lbm_b200 import checkpoint as C
+
+
+def sample(seed=0, n=50, q=19, m=7):
+    r = np.random.default_rng(seed)
+    meta = {"n_nodes": n, "lattice": q, "n_nearwall": m, "storage": "f32", "bc": "physics",
+            "steps": 1234, "runtime": 0.01234}
+    return meta, {"state": r.integers(0, 256, size=5000, dtype=np.uint8)}
+
+
+def test_round_trip(tmp_path):
+    meta, arrays = sample()
+    p = str(tmp_path / "a.ckpt")
+    C.write(p, meta, arrays)
+    got = C.read(p)
+    assert got["meta"] == meta
+    for k, v in arrays.items():
+        np.testing.assert_array_equal(got["arrays"][k], v)
+
+
+def damaged(tmp_path, edit):
+    meta, arrays = sample()
+    p = str(tmp_path / "a.ckpt")
+    C.write(p, meta, arrays)
+    raw = bytearray(open(p, "rb").read())
+    raw = edit(raw)
+    open(p, "wb").write(bytes(raw))
+    return p
+
+
+def header_len(raw):
+    return struct.unpack_from("<Q", raw, len(C.MAGIC))[0]
+
+
+@pytest.mark.parametrize("where", [0.1, 0.5, 0.99])
+def test_flipped_bit_is_a_crc_mismatch(tmp_path, where):
+    def edit(raw):
+        base = len(C.MAGIC) + 8 + header_len(raw)
+        i = base + int(where * (len(raw) - base - 1))
+        raw[i] ^= 0x10
+        return raw
+    with pytest.raises(C.CheckpointError, match="CRC-32 mismatch"):
+        C.read(damaged(tmp_path, edit))
+
+
+def test_truncated_file(tmp_path):
+    with pytest.raises(C.CheckpointError, match="truncated"):
+        C.read(damaged(tmp_path, lambda raw: raw[:-9]))
+    with pytest.raises(C.CheckpointError, match="truncated header"):
+        C.read(damaged(tmp_path, lambda raw: raw[:len(C.MAGIC) + 8 + 5]))
+    with pytest.raises(C.CheckpointError, match="bad magic"):
+        C.read(damaged(tmp_path, lambda raw: raw[:5]))
+
+
+def test_foreign_file_and_trailing_bytes(tmp_path):
+    with pytest.raises(C.CheckpointError, match="bad magic"):
+        C.read(damaged(tmp_path, lambda raw: b"NOTACKPT" + raw[8:]))
+    with pytest.raises(C.CheckpointError, match="after the last array"):
+        C.read(damaged(tmp_path, lambda raw: raw + b"\0\0\0"))
+
+
+def rewrite_header(tmp_path, change):
+    def edit(raw):
+        h = header_len(raw)
+        start = len(C.MAGIC) + 8
+        header = json.loads(bytes(raw[start:start + h]).decode())
+        change(header)
+        new = json.dumps(header).encode()
+        return raw[:len(C.MAGIC)] + struct.pack("<Q", len(new)) + new + raw[start + h:]
+    return damaged(tmp_path, edit)
+
+
+def test_other_version_and_missing_array(tmp_path):
+    with pytest.raises(C.CheckpointError, match="format version"):
+        C.read(rewrite_header(tmp_path, lambda h: h.update(version=99)))
+    with pytest.raises(C.CheckpointError, match="array state missing"):
+        C.read(rewrite_header(tmp_path, lambda h: h["arrays"].pop("state")))
+    with pytest.raises(C.CheckpointError, match="inconsistent"):
+        C.read(rewrite_header(tmp_path, lambda h: h["arrays"]["state"].update(shape=[5001])))
+    with pytest.raises(C.CheckpointError, match="inconsistent"):
+        C.read(rewrite_header(tmp_path, lambda h: h["arrays"]["state"].update(dtype="<f8")))
+
+
+class StandIn:
+    """Records what restore() hands the engine."""
+
+    def __init__(self, n=50, q=19, m=7, storage="f32", bc="physics"):
+        self.n, self.q, self.n_nearwall, self.storage, self.bc = n, q, m, storage, bc
+        self.calls = []
+
+    def set_state(self, blob):
+        self.calls.append(("set_state", blob.dtype.str, blob.shape))
+
+
+def test_restore_hands_over_the_state_and_checks_the_engine(tmp_path):
+    meta, arrays = sample()
+    p = str(tmp_path / "a.ckpt")
+    C.write(p, meta, arrays)
+    ck = C.read(p)
+    e = StandIn()
+    C.restore(e, ck)
+    assert e.calls == [("set_state", "|u1", (5000,))]
+    for bad in (StandIn(storage="f16"), StandIn(bc="reference"), StandIn(n=51), StandIn(q=27), StandIn(m=8)):
+        with pytest.raises(C.CheckpointError):
+            C.restore(bad, ck)
+        assert bad.calls == []
+
+
+def test_state_of_reads_meta_and_blob():
+    fake = types.SimpleNamespace(
+        n=4, q=19, n_nearwall=3, storage="f64", bc="reference",
+        time=lambda: (7, 0.5), get_state=lambda: np.arange(10, dtype=np.uint8))
+    meta, arrays = C.state_of(fake)
+    assert meta == {"n_nodes": 4, "lattice": 19, "n_nearwall": 3, "storage": "f64", "bc": "reference",
+                    "steps": 7, "runtime": 0.5}
+    assert list(arrays) == ["state"]
+    np.testing.assert_array_equal(arrays["state"], np.arange(10, dtype=np.uint8))
+
+
+def test_only_byte_arrays_are_written(tmp_path):
+    meta, _ = sample()
+    with pytest.raises(C.CheckpointError, match="only"):
+        C.write(str(tmp_path / "a.ckpt"), meta, {"state": np.zeros(3)})

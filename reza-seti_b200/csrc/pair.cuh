@@ -349,6 +349,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair0_min_blocks<S, Q>()) pair_p
 // tile's node words and segment offsets into the other half of a
 // double-buffered shared-memory area with cp.async (global -> shared, no
 // registers held). One __syncthreads per tile hands the buffers over.
+// Tiles are taken in descending order: the phase-0 kernel before it sweeps
+// the lattice upwards, so phase 1 starts on the tiles still in L2 from the
+// end of that sweep and ends on tile 0, where the next phase 0 starts.
 
 __device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -425,16 +428,18 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_p
         wait_prior_grid();
         return;
     }
+    // the k-th tile taken is tile n_tiles - 1 - k of the lattice
+    auto lattice_tile = [&](int k) { return n_tiles - 1 - k; };
     int b = 0, sb = 1;
     // node words and segment rows never change: copied before the wait
-    prefetch(tile, 0);
+    prefetch(lattice_tile(tile), 0);
     wait_prior_grid();
     if (tid == 0) sched[0] = gridDim.x + atomicAdd(a.tile_sched, 1);
     cp_async_wait_all();
     __syncthreads();
     int next = sched[0];
     for (;;) {
-        const int n0 = tile * BLOCK_NODES + 2 * tid;
+        const int n0 = lattice_tile(tile) * BLOCK_NODES + 2 * tid;
         const bool live0 = n0 < a.n, live1 = n0 + 1 < a.n;
         const MT m0 = meta_buf(b)[2 * tid];
         const MT m1 = meta_buf(b)[2 * tid + 1];
@@ -449,7 +454,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, pair1_min_blocks<S, Q>()) pair_p
         if (uniform) pair_gather1_twin<S, Q>(a, s, m0, sd0, n0);
         else pair_gather1<S, Q>(a, s, m0, m1, sd0, sd1, n0);
         if (next < n_tiles) {
-            prefetch(next, b ^ 1);
+            prefetch(lattice_tile(next), b ^ 1);
             if (tid == 0) sched[sb] = gridDim.x + atomicAdd(a.tile_sched, 1);
         }
         if (live0) {

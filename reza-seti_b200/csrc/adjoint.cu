@@ -793,9 +793,10 @@ __device__ __forceinline__ void push_pair_body(const AGeom<float, Q>& g, const f
 
 template <int Q>
 __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
-    adj_push_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t) {
+    adj_push_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t,
+                         int rev) {
     allow_next_grid();
-    push_pair_body<Q>(g, D, Dn, s_t, blockIdx.x);
+    push_pair_body<Q>(g, D, Dn, s_t, rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x);
 }
 
 // The forward sweep's objective term and push of one step in one launch: the
@@ -806,14 +807,15 @@ __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
 template <int Q, bool THREADS>
 __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PUSH_MIN_BLOCKS)
     adj_push_objective_kernel(AGeom<float, Q> g, const float* __restrict__ D, float* __restrict__ Dn, double s_t,
-                              ObjArgs<float, Q> a, int t, int obj_blocks) {
+                              ObjArgs<float, Q> a, int t, int obj_blocks, int rev) {
     allow_next_grid();
     if ((int)blockIdx.x < obj_blocks) {
         wait_prior_grid();
         if (THREADS) objective_thread_body<float, Q>(a, D, t, blockIdx.x);
         else objective_warp_body<float, Q>(a, D, t, blockIdx.x);
     } else {
-        push_pair_body<Q>(g, D, Dn, s_t, (int)blockIdx.x - obj_blocks);
+        const int b = (int)blockIdx.x - obj_blocks, nb = (int)gridDim.x - obj_blocks;
+        push_pair_body<Q>(g, D, Dn, s_t, rev ? nb - 1 - b : b);
     }
 }
 
@@ -1072,9 +1074,10 @@ template <int Q>
 __global__ void __launch_bounds__(PAIR_THREADS, LBM_ADJ_PULL_MIN_BLOCKS)
     adj_pull_pair_kernel(AGeom<float, Q> g, const float* __restrict__ D, const float* __restrict__ Ln,
                          float* __restrict__ Lc, double s_t, double* __restrict__ dspeed,
-                         double* __restrict__ domega, const float* __restrict__ Gadd) {
+                         double* __restrict__ domega, const float* __restrict__ Gadd, int rev) {
     allow_next_grid();
-    pull_pair_body<Q>(g, D, Ln, Lc, s_t, dspeed, domega, Gadd, blockIdx.x);
+    pull_pair_body<Q>(g, D, Ln, Lc, s_t, dspeed, domega, Gadd,
+                      rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x);
 }
 
 struct Arena {
@@ -1267,7 +1270,7 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
                 const cudaError_t e = launch_pdl(adj_push_pair_kernel<Q>, pgrid, dim3(PAIR_THREADS), 0, stream, g, D,
-                                                 Dn, s.factors[t]);
+                                                 Dn, s.factors[t], (int)(t & 1));
                 (void)e;  // launch errors surface through cudaGetLastError after the sweep
                 return;
             }
@@ -1279,7 +1282,8 @@ int run(const AdjointSetup& s, AdjointOut& o) {
         if constexpr (std::is_same<R, float>::value) {
             if (pairs) {
                 const cudaError_t e = launch_pdl(adj_pull_pair_kernel<Q>, pgrid, dim3(PAIR_THREADS), (size_t)pull_smem, st,
-                                                 g, D, Ln, Lc, s.factors[t], dspeed, scal + N_PARTIALS, Gadd);
+                                                 g, D, Ln, Lc, s.factors[t], dspeed, scal + N_PARTIALS, Gadd,
+                                                 (int)(t & 1));
                 (void)e;  // launch errors surface through cudaGetLastError after the sweep
                 return;
             }
@@ -1300,10 +1304,10 @@ int run(const AdjointSetup& s, AdjointOut& o) {
                 cudaError_t e;
                 if (obj_threads)
                     e = launch_pdl(adj_push_objective_kernel<Q, true>, fgrid, dim3(PAIR_THREADS), 0, st, g, D, Dn,
-                                   s.factors[t], oa, (int)t, ob);
+                                   s.factors[t], oa, (int)t, ob, (int)(t & 1));
                 else
                     e = launch_pdl(adj_push_objective_kernel<Q, false>, fgrid, dim3(PAIR_THREADS), 0, st, g, D, Dn,
-                                   s.factors[t], oa, (int)t, ob);
+                                   s.factors[t], oa, (int)t, ob, (int)(t & 1));
                 (void)e;  // launch errors surface through cudaGetLastError after the sweep
                 return;
             }

@@ -1,8 +1,9 @@
 """Checkpoint files: stop a run and resume it bit for bit.
 
 The reference writes no restart files; its only outputs are the result files
-of Simulation::WriteOutput (Simulation.cpp:835-856). A checkpoint here holds
-the engine's state blob (lbm_get_state): the stored populations in the storage
+of Simulation::WriteOutput (Simulation.cpp:835-856). An engine checkpoint
+holds the engine's state blob (lbm_get_state), and a slab-set checkpoint holds
+one blob per slab engine. A blob carries the stored populations in the storage
 type, the near-wall moments the next wall shear stress uses, the WSS with its
 FP64 accumulators, the step count, the flow clock and the AA phase. FP64
 populations would not do for the 16-bit and FP32 storage types: f = w + d
@@ -17,7 +18,7 @@ File layout, all little-endian:
 * the header length as a uint64;
 * a JSON header: format version, engine settings, step count and clock, and
   per array its dtype, shape, byte offset, length and CRC-32;
-* the arrays' raw bytes.
+* the arrays' raw bytes, one after another.
 read() checks the magic, the header, and every array's length and CRC-32. It
 raises CheckpointError naming the first thing that is wrong, before anything
 reaches an engine.
@@ -33,8 +34,10 @@ import numpy as np
 
 MAGIC = b"LBMCKPT1"
 VERSION = 1
-ARRAYS = ("state",)
 DTYPES = {"|u1": 1}
+# the arrays each kind of checkpoint must hold
+REQUIRED = {"engine": lambda meta: ["state"],
+            "slab_set": lambda meta: ["state_%d" % r for r in range(int(meta.get("n_slabs", 0)))]}
 
 
 class CheckpointError(ValueError):
@@ -45,16 +48,19 @@ class CheckpointError(ValueError):
 def state_of(engine):
     """(meta, arrays) of an engine's current state."""
     steps, runtime = engine.time()
-    meta = {"n_nodes": int(engine.n), "lattice": int(engine.q), "n_nearwall": int(engine.n_nearwall),
-            "storage": engine.storage, "bc": engine.bc, "steps": int(steps), "runtime": float(runtime)}
+    meta = {"kind": "engine", "n_nodes": int(engine.n), "lattice": int(engine.q),
+            "n_nearwall": int(engine.n_nearwall), "storage": engine.storage, "bc": engine.bc,
+            "steps": int(steps), "runtime": float(runtime)}
     return meta, {"state": engine.get_state()}
 
 
 def write(path, meta, arrays):
     """Writes meta and the arrays to path (through a temporary file that
     replaces path once complete)."""
+    if not arrays:
+        raise CheckpointError("nothing to write")
     entries, blobs, offset = {}, [], 0
-    for name in ARRAYS:
+    for name in arrays:
         a = np.ascontiguousarray(arrays[name])
         dt = a.dtype.str
         if dt not in DTYPES:
@@ -100,13 +106,18 @@ def read(path):
         raise CheckpointError("%s: format version %r, this reader takes %d"
                               % (path, header.get("version") if isinstance(header, dict) else None, VERSION))
     meta, entries = header.get("meta"), header.get("arrays")
-    if not isinstance(meta, dict) or not isinstance(entries, dict):
+    if not isinstance(meta, dict) or not isinstance(entries, dict) or not entries:
         raise CheckpointError("%s: header without meta or arrays" % path)
-    base, end, arrays = start + hlen, start + hlen, {}
-    for name in ARRAYS:
-        e = entries.get(name)
-        if not isinstance(e, dict):
+    kind = meta.get("kind")
+    if kind not in REQUIRED:
+        raise CheckpointError("%s: unknown kind of checkpoint %r" % (path, kind))
+    for name in REQUIRED[kind](meta):
+        if name not in entries:
             raise CheckpointError("%s: array %s missing" % (path, name))
+    base, end, arrays, spans = start + hlen, start + hlen, {}, []
+    for name, e in entries.items():
+        if not isinstance(e, dict):
+            raise CheckpointError("%s: bad entry for array %s" % (path, name))
         try:
             lo, n, shape, crc = base + int(e["offset"]), int(e["nbytes"]), [int(x) for x in e["shape"]], int(e["crc32"])
         except (KeyError, TypeError, ValueError):
@@ -120,7 +131,14 @@ def read(path):
         if zlib.crc32(b) != crc:
             raise CheckpointError("%s: CRC-32 mismatch in array %s" % (path, name))
         arrays[name] = np.frombuffer(b, dtype=dt).reshape(shape).copy()
+        spans.append((lo, n, name))
         end = max(end, lo + n)
+    # the arrays tile the payload: no overlap, no gap
+    at = base
+    for lo, n, name in sorted(spans):
+        if lo != at:
+            raise CheckpointError("%s: array %s does not start where the previous one ends" % (path, name))
+        at = lo + n
     if end != len(data):
         raise CheckpointError("%s: %d bytes after the last array" % (path, len(data) - end))
     return {"meta": meta, "arrays": arrays}
@@ -128,7 +146,7 @@ def read(path):
 
 def check_compatible(engine, meta):
     """Raises CheckpointError unless engine matches the one that wrote meta."""
-    mine = {"n_nodes": engine.n, "lattice": engine.q, "n_nearwall": engine.n_nearwall,
+    mine = {"kind": "engine", "n_nodes": engine.n, "lattice": engine.q, "n_nearwall": engine.n_nearwall,
             "storage": engine.storage, "bc": engine.bc}
     for k, v in mine.items():
         if meta.get(k) != v:
@@ -142,3 +160,28 @@ def restore(engine, ckpt):
     meta, arrays = ckpt["meta"], ckpt["arrays"]
     check_compatible(engine, meta)
     engine.set_state(arrays["state"])
+
+
+def slab_set_state(slab_set):
+    """(meta, arrays) of a SlabSet (lbm_b200.slabs): every slab engine's state."""
+    engines = slab_set.engines
+    steps, runtime = engines[0].time()
+    meta = {"kind": "slab_set", "n_slabs": len(engines), "n_nodes": int(slab_set.n), "lattice": int(slab_set.q),
+            "storage": engines[0].storage, "steps": int(steps), "runtime": float(runtime),
+            "slab_nodes": [int(e.n) for e in engines]}
+    return meta, {"state_%d" % r: e.get_state() for r, e in enumerate(engines)}
+
+
+def restore_slab_set(slab_set, ckpt):
+    """Puts a slab-set checkpoint into slab_set, which must cut the same
+    lattice into the same slabs with the same storage type."""
+    meta, arrays = ckpt["meta"], ckpt["arrays"]
+    engines = slab_set.engines
+    mine = {"kind": "slab_set", "n_slabs": len(engines), "n_nodes": slab_set.n, "lattice": slab_set.q,
+            "storage": engines[0].storage, "slab_nodes": [e.n for e in engines]}
+    for k, v in mine.items():
+        if meta.get(k) != v:
+            raise CheckpointError("checkpoint %s is %r, the slab set's %r" % (k, meta.get(k), v))
+    for r, e in enumerate(engines):
+        e.set_state(arrays["state_%d" % r])
+

@@ -296,6 +296,21 @@ class SlabSet:
                 e.step(1)
             self.exchange()
 
+    # ---- checkpoint and resume
+    def save_checkpoint(self, path):
+        """Writes every slab engine's state to one checkpoint file."""
+        from . import checkpoint
+        checkpoint.write(path, *checkpoint.slab_set_state(self))
+
+    def load_checkpoint(self, path):
+        """Restores a checkpoint of a slab set cut the same way, after the flow
+        settings. The halo exchange runs again before the next step. It copies
+        the values the checkpointed set had already exchanged, so the steps
+        continue bit for bit."""
+        from . import checkpoint
+        checkpoint.restore_slab_set(self, checkpoint.read(path))
+        self._synced = False
+
     # ---- results in the whole lattice's order
     def populations(self):
         f = np.empty((self.n, self.q))
@@ -389,6 +404,21 @@ class SlabRank:
 
     def mark_stale(self):
         """After a setter that re-initialised the engine's store."""
+        self._synced = False
+
+    def checkpoint_path(self, path):
+        """This rank's file of a checkpoint written by every rank."""
+        return "%s.slab%d" % (path, self.slab.rank)
+
+    def save_checkpoint(self, path):
+        """Every rank writes its engine's state to checkpoint_path(path)."""
+        self.engine.save_checkpoint(self.checkpoint_path(path))
+
+    def load_checkpoint(self, path):
+        """Every rank restores its engine from checkpoint_path(path); the halo
+        exchange runs again before the next step (it copies what the
+        checkpointed ranks had already exchanged)."""
+        self.engine.load_checkpoint(self.checkpoint_path(path))
         self._synced = False
 
     def step(self, n=1):

@@ -16,7 +16,7 @@ from lbm_b200 import checkpoint as C
 
 def sample(seed=0, n=50, q=19, m=7):
     r = np.random.default_rng(seed)
-    meta = {"n_nodes": n, "lattice": q, "n_nearwall": m, "storage": "f32", "bc": "physics",
+    meta = {"kind": "engine", "n_nodes": n, "lattice": q, "n_nearwall": m, "storage": "f32", "bc": "physics",
             "steps": 1234, "runtime": 0.01234}
     return meta, {"state": r.integers(0, 256, size=5000, dtype=np.uint8)}
 
@@ -86,8 +86,10 @@ def rewrite_header(tmp_path, change):
 def test_other_version_and_missing_array(tmp_path):
     with pytest.raises(C.CheckpointError, match="format version"):
         C.read(rewrite_header(tmp_path, lambda h: h.update(version=99)))
-    with pytest.raises(C.CheckpointError, match="array state missing"):
+    with pytest.raises(C.CheckpointError, match="without meta or arrays"):
         C.read(rewrite_header(tmp_path, lambda h: h["arrays"].pop("state")))
+    with pytest.raises(C.CheckpointError, match="array state missing"):
+        C.read(rewrite_header(tmp_path, lambda h: h["arrays"].update(other=h["arrays"].pop("state"))))
     with pytest.raises(C.CheckpointError, match="inconsistent"):
         C.read(rewrite_header(tmp_path, lambda h: h["arrays"]["state"].update(shape=[5001])))
     with pytest.raises(C.CheckpointError, match="inconsistent"):
@@ -124,8 +126,8 @@ def test_state_of_reads_meta_and_blob():
         n=4, q=19, n_nearwall=3, storage="f64", bc="reference",
         time=lambda: (7, 0.5), get_state=lambda: np.arange(10, dtype=np.uint8))
     meta, arrays = C.state_of(fake)
-    assert meta == {"n_nodes": 4, "lattice": 19, "n_nearwall": 3, "storage": "f64", "bc": "reference",
-                    "steps": 7, "runtime": 0.5}
+    assert meta == {"kind": "engine", "n_nodes": 4, "lattice": 19, "n_nearwall": 3, "storage": "f64",
+                    "bc": "reference", "steps": 7, "runtime": 0.5}
     assert list(arrays) == ["state"]
     np.testing.assert_array_equal(arrays["state"], np.arange(10, dtype=np.uint8))
 
@@ -134,3 +136,59 @@ def test_only_byte_arrays_are_written(tmp_path):
     meta, _ = sample()
     with pytest.raises(C.CheckpointError, match="only"):
         C.write(str(tmp_path / "a.ckpt"), meta, {"state": np.zeros(3)})
+
+
+def test_unknown_kind_and_overlapping_arrays(tmp_path):
+    with pytest.raises(C.CheckpointError, match="unknown kind"):
+        C.read(rewrite_header(tmp_path, lambda h: h["meta"].update(kind="something")))
+
+    def two_arrays(h):
+        # a second array claiming the first one's bytes
+        h["arrays"]["extra"] = dict(h["arrays"]["state"])
+    with pytest.raises(C.CheckpointError, match="does not start"):
+        C.read(rewrite_header(tmp_path, two_arrays))
+
+
+class SlabEngine(StandIn):
+    def __init__(self, n, blob_len):
+        super().__init__(n=n)
+        self.blob_len = blob_len
+
+    def time(self):
+        return (40, 0.0)
+
+    def get_state(self):
+        return np.full(self.blob_len, self.n % 251, dtype=np.uint8)
+
+
+def test_slab_set_round_trip_and_checks(tmp_path):
+    eng = [SlabEngine(30, 100), SlabEngine(25, 90), SlabEngine(28, 96)]
+    ss = types.SimpleNamespace(engines=eng, n=80, q=19)
+    meta, arrays = C.slab_set_state(ss)
+    assert meta["kind"] == "slab_set" and meta["n_slabs"] == 3 and meta["slab_nodes"] == [30, 25, 28]
+    p = str(tmp_path / "s.ckpt")
+    C.write(p, meta, arrays)
+    ck = C.read(p)
+    fresh = [SlabEngine(30, 100), SlabEngine(25, 90), SlabEngine(28, 96)]
+    C.restore_slab_set(types.SimpleNamespace(engines=fresh, n=80, q=19), ck)
+    assert [e.calls for e in fresh] == [[("set_state", "|u1", (100,))], [("set_state", "|u1", (90,))],
+                                        [("set_state", "|u1", (96,))]]
+    # another cut of the lattice is refused before any engine is touched
+    other = [SlabEngine(30, 100), SlabEngine(26, 90), SlabEngine(27, 96)]
+    with pytest.raises(C.CheckpointError, match="slab_nodes"):
+        C.restore_slab_set(types.SimpleNamespace(engines=other, n=80, q=19), ck)
+    assert all(e.calls == [] for e in other)
+    # an engine checkpoint is not a slab-set checkpoint, nor the other way round
+    with pytest.raises(C.CheckpointError, match="kind"):
+        C.restore(StandIn(), ck)
+    with pytest.raises(C.CheckpointError, match="array state_2 missing"):
+        C.read(rewrite_slab_header(tmp_path, ss))
+
+
+def rewrite_slab_header(tmp_path, ss):
+    meta, arrays = C.slab_set_state(ss)
+    arrays.pop("state_2")
+    p = str(tmp_path / "short.ckpt")
+    C.write(p, meta, arrays)
+    return p
+

@@ -72,6 +72,16 @@ class AAEmulator:
                     f[opp[p], nodes[~have]] = c[p, ~have]
             self.phase ^= 1
 
+    # the engine's checkpoint interface (its whole state: slots and phase)
+    def save_checkpoint(self, path):
+        with open(path, "wb") as fh:
+            np.savez(fh, f=self.f, phase=self.phase)
+
+    def load_checkpoint(self, path):
+        with np.load(path) as d:
+            self.f = d["f"].copy()
+            self.phase = int(d["phase"])
+
     # the engine's halo interface
     def next_phase(self):
         return self.phase
@@ -195,6 +205,57 @@ def rank_main(rank, world, port, out):
         dist.barrier()
     finally:
         dist.destroy_process_group()
+
+
+def rank_resume_main(rank, world, port, out, ckdir):
+    """5 steps, a checkpoint, then a new rank object with a fresh engine
+    restores it and takes 4 more steps."""
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "reza-seti_b200"))
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from lbm_b200 import slabs as SS
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        topo = small_pipe()
+        slab = SS.partition(topo, world, lattice=19)[rank]
+        r = SS.SlabRank(slab, AAEmulator(slab.topo["coords"], 19), device="cpu", dtype=torch.float64)
+        r.step(5)
+        path = os.path.join(ckdir, "run")
+        r.save_checkpoint(path)
+        emu = AAEmulator(slab.topo["coords"], 19, seed=11)  # another initial state
+        r2 = SS.SlabRank(slab, emu, device="cpu", dtype=torch.float64)
+        r2.load_checkpoint(path)
+        r2.step(4)
+        out.put((rank, slab.owned, emu.f[:, :slab.n_owned].copy(), os.path.exists(r.checkpoint_path(path))))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_resume_from_checkpoint(tmp_path):
+    """Each rank restores its own checkpoint file into a fresh engine; the
+    exchange that SlabRank runs again before the next step makes the resumed
+    run equal the undivided lattice's 9 steps."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=rank_resume_main, args=(r, 2, port, q, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    topo = small_pipe()
+    full = AAEmulator(topo["coords"], 19)
+    full.step(9)
+    for rank, owned, f, wrote in got:
+        assert wrote
+        np.testing.assert_array_equal(f, full.f[:, owned])
+    assert sorted(os.listdir(tmp_path)) == ["run.slab0", "run.slab1"]
 
 
 def test_two_gloo_ranks_equal_whole_lattice():

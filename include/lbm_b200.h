@@ -165,8 +165,8 @@ int lbm_get_time(lbm_engine* e, int64_t* steps, double* runtime);
  * moments and fluxes are readable again after the next step (LBM_ERR_STATE
  * before it); WSS and OSI/TAWSS at once. */
 int lbm_state_size(lbm_engine* e, int64_t* bytes);
-int lbm_get_state(lbm_engine* e, void* dst);
-int lbm_set_state(lbm_engine* e, const void* src);
+int lbm_get_state(lbm_engine* e, void* dst, int64_t dst_bytes);   /* dst_bytes >= the size */
+int lbm_set_state(lbm_engine* e, const void* src, int64_t src_bytes);  /* src_bytes == the size */
 
 /* Node::m_distributions after the last step (post-boundary populations),
  * [n_nodes][q] in the caller's node order. */

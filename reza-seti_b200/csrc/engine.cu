@@ -1155,11 +1155,14 @@ int lbm_state_size(lbm_engine* e, int64_t* bytes) {
     return 0;
 }
 
-int lbm_get_state(lbm_engine* e, void* dst) {
+int lbm_get_state(lbm_engine* e, void* dst, int64_t bytes) {
     if (!e || !dst) return LBM_ERR_ARGUMENT;
     if (e->wss_pending) return e->fail(LBM_ERR_STATE, "lbm_get_state: a wall shear stress reduction is pending");
-    cudaSetDevice(e->device);
     const StateHeader h = state_header(e);
+    if (bytes < state_bytes(h))
+        return e->fail(LBM_ERR_ARGUMENT, "lbm_get_state: buffer of " + std::to_string(bytes) +
+                                             " bytes, the state needs " + std::to_string(state_bytes(h)));
+    cudaSetDevice(e->device);
     char* p = static_cast<char*>(dst);
     std::memcpy(p, &h, sizeof h);
     p += sizeof h;
@@ -1177,11 +1180,14 @@ int lbm_get_state(lbm_engine* e, void* dst) {
     return sync(e);
 }
 
-int lbm_set_state(lbm_engine* e, const void* src) {
+int lbm_set_state(lbm_engine* e, const void* src, int64_t bytes) {
     if (!e || !src) return LBM_ERR_ARGUMENT;
+    const StateHeader mine = state_header(e);
+    if (bytes != state_bytes(mine))
+        return e->fail(LBM_ERR_ARGUMENT, "lbm_set_state: blob of " + std::to_string(bytes) +
+                                             " bytes, this engine's state has " + std::to_string(state_bytes(mine)));
     StateHeader h;
     std::memcpy(&h, src, sizeof h);
-    const StateHeader mine = state_header(e);
     if (h.magic != STATE_MAGIC || h.version != STATE_VERSION)
         return e->fail(LBM_ERR_ARGUMENT, "lbm_set_state: not a state blob of this version");
     if (h.lattice != mine.lattice || h.storage != mine.storage || h.bc != mine.bc || h.n != mine.n ||
@@ -1190,7 +1196,8 @@ int lbm_set_state(lbm_engine* e, const void* src) {
         return e->fail(LBM_ERR_ARGUMENT,
                        "lbm_set_state: the state comes from an engine with another node set, lattice, "
                        "storage type or boundary mode");
-    if (h.phase != 0 && h.phase != 1) return e->fail(LBM_ERR_ARGUMENT, "lbm_set_state: bad phase");
+    if ((h.phase != 0 && h.phase != 1) || h.step < 0 || !std::isfinite(h.runtime))
+        return e->fail(LBM_ERR_ARGUMENT, "lbm_set_state: bad phase, step or clock");
     cudaSetDevice(e->device);
     if (int rc = sync(e)) return rc;
     const char* p = static_cast<const char*>(src) + sizeof h;

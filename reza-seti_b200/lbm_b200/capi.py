@@ -136,8 +136,8 @@ SIGNATURES = {
     "lbm_set_numeric_check": (ctypes.c_int, [_E, ctypes.c_int32]),
     "lbm_get_time": (ctypes.c_int, [_E, _i64p, _f64p]),
     "lbm_state_size": (ctypes.c_int, [_E, _i64p]),
-    "lbm_get_state": (ctypes.c_int, [_E, ctypes.c_void_p]),
-    "lbm_set_state": (ctypes.c_int, [_E, ctypes.c_void_p]),
+    "lbm_get_state": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_int64]),
+    "lbm_set_state": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_int64]),
     "lbm_get_populations": (ctypes.c_int, [_E, ctypes.c_void_p]),
     "lbm_set_populations": (ctypes.c_int, [_E, ctypes.c_void_p]),
     "lbm_get_macros": (ctypes.c_int, [_E, ctypes.c_void_p, ctypes.c_void_p]),

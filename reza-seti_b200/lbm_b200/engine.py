@@ -184,18 +184,14 @@ class Engine:
         size = ctypes.c_int64()
         self._check(capi.lib().lbm_state_size(self._h, ctypes.byref(size)))
         buf = np.empty(size.value, dtype=np.uint8)
-        self._check(capi.lib().lbm_get_state(self._h, buf.ctypes.data))
+        self._check(capi.lib().lbm_get_state(self._h, buf.ctypes.data, buf.size))
         return buf
 
     def set_state(self, blob):
         """Restores a state from get_state of an engine like this one
         (lbm_set_state); the steps then continue bit for bit."""
-        size = ctypes.c_int64()
-        self._check(capi.lib().lbm_state_size(self._h, ctypes.byref(size)))
         buf = np.ascontiguousarray(blob, dtype=np.uint8).reshape(-1)
-        if buf.size != size.value:
-            raise ValueError("state of %d bytes, this engine's is %d" % (buf.size, size.value))
-        self._check(capi.lib().lbm_set_state(self._h, buf.ctypes.data))
+        self._check(capi.lib().lbm_set_state(self._h, buf.ctypes.data, buf.size))
 
     def populations(self, out=None):
         f = np.empty((self.n, self.q)) if out is None else out

@@ -108,6 +108,13 @@ def test_set_state_refuses_a_foreign_blob():
     bad[0] ^= 0xFF
     with pytest.raises(LbmError, match="not a state blob"):
         a.set_state(bad)
+    # the C ABI checks the length it is given, both ways
+    with pytest.raises(LbmError, match="bytes"):
+        a.set_state(blob[:-1])
+    from lbm_b200 import capi
+    short = np.empty(blob.size - 1, dtype=np.uint8)
+    with pytest.raises(LbmError, match="buffer of"):
+        capi.check(capi.lib().lbm_get_state(a._h, short.ctypes.data, short.size), a._h)
     a.close()
     b.close()
 

@@ -14,26 +14,28 @@ engine from the same topology with the same settings, then call restore():
 the steps taken from there equal those of the run that was never stopped.
 
 File layout, all little-endian:
-* the 8-byte magic b"LBMCKPT1";
-* the header length as a uint64;
+* the 8-byte magic b"LBMCKPT2";
+* the header length as a uint64 and the header's CRC-32 as a uint32;
 * a JSON header: format version, engine settings, step count and clock, and
   per array its dtype, shape, byte offset, length and CRC-32;
 * the arrays' raw bytes, one after another.
-read() checks the magic, the header, and every array's length and CRC-32. It
-raises CheckpointError naming the first thing that is wrong, before anything
-reaches an engine.
+read() checks the magic, the header's CRC-32 and contents, and every array's
+length and CRC-32. It raises CheckpointError naming the first thing that is
+wrong, before anything reaches an engine.
 """
 from __future__ import annotations
 
 import json
+import math
 import os
 import struct
 import zlib
 
 import numpy as np
 
-MAGIC = b"LBMCKPT1"
-VERSION = 1
+MAGIC = b"LBMCKPT2"
+VERSION = 2
+PREFIX = struct.Struct("<QI")  # header length, header CRC-32
 DTYPES = {"|u1": 1}
 # the arrays each kind of checkpoint must hold
 REQUIRED = {"engine": lambda meta: ["state"],
@@ -74,7 +76,7 @@ def write(path, meta, arrays):
     tmp = path + ".tmp"
     with open(tmp, "wb") as fh:
         fh.write(MAGIC)
-        fh.write(struct.pack("<Q", len(header)))
+        fh.write(PREFIX.pack(len(header), zlib.crc32(header)))
         fh.write(header)
         for b in blobs:
             fh.write(b)
@@ -92,12 +94,14 @@ def read(path):
     """{"meta": ..., "arrays": ...} of a checkpoint file, every array checked."""
     with open(path, "rb") as fh:
         data = fh.read()
-    start = len(MAGIC) + 8
+    start = len(MAGIC) + PREFIX.size
     if len(data) < start or data[: len(MAGIC)] != MAGIC:
         raise CheckpointError("%s: not a checkpoint file (bad magic)" % path)
-    (hlen,) = struct.unpack_from("<Q", data, len(MAGIC))
+    hlen, hcrc = PREFIX.unpack_from(data, len(MAGIC))
     if start + hlen > len(data):
         raise CheckpointError("%s: truncated header" % path)
+    if zlib.crc32(data[start:start + hlen]) != hcrc:
+        raise CheckpointError("%s: CRC-32 mismatch in the header" % path)
     try:
         header = json.loads(data[start:start + hlen].decode())
     except (UnicodeDecodeError, ValueError) as exc:
@@ -123,7 +127,8 @@ def read(path):
         except (KeyError, TypeError, ValueError):
             raise CheckpointError("%s: bad entry for array %s" % (path, name)) from None
         dt = e.get("dtype")
-        if dt not in DTYPES or n != DTYPES[dt] * int(np.prod(shape)) or lo < base:
+        if (dt not in DTYPES or any(d < 0 for d in shape) or n != DTYPES[dt] * math.prod(shape)
+                or lo < base):
             raise CheckpointError("%s: array %s: shape, type or offset inconsistent" % (path, name))
         if lo + n > len(data):
             raise CheckpointError("%s: truncated in array %s" % (path, name))

@@ -5,8 +5,8 @@ format version, trailing bytes, a missing array. Also checked: a checkpoint is
 refused by an engine unlike its writer, and restore() hands the engine the
 state blob. A stand-in records the calls; no GPU is used."""
 import json
-import struct
 import types
+import zlib
 
 import numpy as np
 import pytest
@@ -42,13 +42,16 @@ def damaged(tmp_path, edit):
 
 
 def header_len(raw):
-    return struct.unpack_from("<Q", raw, len(C.MAGIC))[0]
+    return C.PREFIX.unpack_from(raw, len(C.MAGIC))[0]
+
+
+HEADER_START = len(C.MAGIC) + C.PREFIX.size
 
 
 @pytest.mark.parametrize("where", [0.1, 0.5, 0.99])
 def test_flipped_bit_is_a_crc_mismatch(tmp_path, where):
     def edit(raw):
-        base = len(C.MAGIC) + 8 + header_len(raw)
+        base = HEADER_START + header_len(raw)
         i = base + int(where * (len(raw) - base - 1))
         raw[i] ^= 0x10
         return raw
@@ -60,7 +63,7 @@ def test_truncated_file(tmp_path):
     with pytest.raises(C.CheckpointError, match="truncated"):
         C.read(damaged(tmp_path, lambda raw: raw[:-9]))
     with pytest.raises(C.CheckpointError, match="truncated header"):
-        C.read(damaged(tmp_path, lambda raw: raw[:len(C.MAGIC) + 8 + 5]))
+        C.read(damaged(tmp_path, lambda raw: raw[:HEADER_START + 5]))
     with pytest.raises(C.CheckpointError, match="bad magic"):
         C.read(damaged(tmp_path, lambda raw: raw[:5]))
 
@@ -73,14 +76,24 @@ def test_foreign_file_and_trailing_bytes(tmp_path):
 
 
 def rewrite_header(tmp_path, change):
+    """A file whose header is changed and re-checksummed: what only the
+    content checks can catch."""
     def edit(raw):
         h = header_len(raw)
-        start = len(C.MAGIC) + 8
-        header = json.loads(bytes(raw[start:start + h]).decode())
+        header = json.loads(bytes(raw[HEADER_START:HEADER_START + h]).decode())
         change(header)
         new = json.dumps(header).encode()
-        return raw[:len(C.MAGIC)] + struct.pack("<Q", len(new)) + new + raw[start + h:]
+        return raw[:len(C.MAGIC)] + C.PREFIX.pack(len(new), zlib.crc32(new)) + new + raw[HEADER_START + h:]
     return damaged(tmp_path, edit)
+
+
+def test_header_is_checksummed(tmp_path):
+    def edit(raw):
+        i = HEADER_START + header_len(raw) // 2
+        raw[i] ^= 0x01
+        return raw
+    with pytest.raises(C.CheckpointError, match="CRC-32 mismatch in the header"):
+        C.read(damaged(tmp_path, edit))
 
 
 def test_other_version_and_missing_array(tmp_path):
@@ -192,3 +205,47 @@ def rewrite_slab_header(tmp_path, ss):
     C.write(p, meta, arrays)
     return p
 
+
+
+def test_any_corruption_is_refused_or_harmless(tmp_path):
+    """Seeded fuzzing of the reader: whatever bytes change, go missing or get
+    inserted, read() raises CheckpointError or returns exactly the content
+    written (a change that JSON ignores, such as one kind of whitespace for
+    another). It never fails another way."""
+    meta, arrays = sample(n=20, m=3)
+    p = str(tmp_path / "a.ckpt")
+    C.write(p, meta, arrays)
+    good = open(p, "rb").read()
+    rng = np.random.default_rng(2024)
+    outcomes = {"refused": 0, "same": 0}
+    for trial in range(400):
+        raw = bytearray(good)
+        kind = trial % 4
+        if kind == 0:      # flip one byte anywhere
+            i = int(rng.integers(len(raw)))
+            raw[i] ^= int(rng.integers(1, 256))
+        elif kind == 1:    # flip one byte of the header
+            i = int(rng.integers(len(C.MAGIC), HEADER_START + header_len(good)))
+            raw[i] ^= int(rng.integers(1, 256))
+        elif kind == 2:    # cut the file short
+            raw = raw[:int(rng.integers(len(raw)))]
+        else:              # insert bytes
+            i = int(rng.integers(len(raw) + 1))
+            raw[i:i] = bytes(rng.integers(0, 256, size=int(rng.integers(1, 9)), dtype=np.uint8))
+        q = str(tmp_path / "b.ckpt")
+        open(q, "wb").write(bytes(raw))
+        try:
+            got = C.read(q)
+        except C.CheckpointError:
+            outcomes["refused"] += 1
+            continue
+        assert got["meta"] == meta
+        np.testing.assert_array_equal(got["arrays"]["state"], arrays["state"])
+        outcomes["same"] += 1
+    assert outcomes["refused"] > 300
+
+
+def test_hostile_shapes_are_refused(tmp_path):
+    for shape in ([-5000, -1], [2 ** 40, 2 ** 40], [5000, 0]):
+        with pytest.raises(C.CheckpointError, match="inconsistent"):
+            C.read(rewrite_header(tmp_path, lambda h: h["arrays"]["state"].update(shape=shape)))

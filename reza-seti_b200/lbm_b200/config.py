@@ -29,7 +29,9 @@ SMOOTHING_RADIUS = 0.25
 
 
 def _str(b):
-    return bytes(b).split(b"\0", 1)[0].decode()
+    # the reference keeps these fields as raw std::string bytes: decode as
+    # file names are, so bytes that are not UTF-8 survive (and still open)
+    return os.fsdecode(bytes(b).split(b"\0", 1)[0])
 
 
 def read_config(path):

@@ -98,3 +98,50 @@ def test_struct_layouts_match_header(tmp_path):
     subprocess.run([cc, "-I", os.path.dirname(capi.HEADER_PATH), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert got == want
+
+
+def header_prototypes():
+    """{name: (return type, [parameter declarations])} from the header."""
+    text = open(capi.HEADER_PATH).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"^\s*#.*$", "", text, flags=re.M)  # preprocessor lines
+    protos = {}
+    for ret, name, params in re.findall(r"([A-Za-z_][\w\s\*]*?)\b(lbm_[a-z_]+)\s*\(([^;{]*?)\)\s*;", text):
+        p = [x.strip() for x in params.split(",")] if params.strip() not in ("", "void") else []
+        protos[name] = (" ".join(ret.split()), p)
+    return protos
+
+
+def c_kind(decl):
+    """The kind of value a C declaration passes: pointer or an integer or
+    floating type of a given size."""
+    if "*" in decl or "[" in decl:  # an array parameter is a pointer
+        return "pointer"
+    t = decl.replace("const ", "").split()[0]
+    return {"int": "i32", "int32_t": "i32", "uint32_t": "u32", "int64_t": "i64", "size_t": "u64",
+            "double": "f64", "float": "f32"}[t]
+
+
+def ctypes_kind(t):
+    if t in (ctypes.c_void_p, ctypes.c_char_p) or (isinstance(t, type) and issubclass(t, ctypes._Pointer)):
+        return "pointer"
+    return {ctypes.c_int32: "i32", ctypes.c_uint32: "u32", ctypes.c_int64: "i64", ctypes.c_uint64: "u64",
+            ctypes.c_double: "f64", ctypes.c_float: "f32"}[t]
+
+
+def test_binding_signatures_match_header_prototypes():
+    """Each entry point's ctypes signature passes the same number and kinds of
+    arguments as its prototype in include/lbm_b200.h, and its return value
+    has the prototype's kind: a parameter added on one side only fails
+    here, without a GPU."""
+    protos = header_prototypes()
+    assert sorted(protos) == sorted(capi.SIGNATURES)
+    for name, (res, args) in capi.SIGNATURES.items():
+        ret, params = protos[name]
+        assert len(params) == len(args), (name, params)
+        for decl, t in zip(params, args):
+            assert c_kind(decl) == ctypes_kind(t), (name, decl, t)
+        if ret == "void":
+            assert res is None, (name, res)
+        else:
+            assert ("pointer" if "*" in ret else c_kind(ret)) == ctypes_kind(res), (name, ret, res)
